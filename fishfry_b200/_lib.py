@@ -1,0 +1,110 @@
+"""ctypes binding of the fishfry_b200 C ABI (include/fishfry.h).
+
+The native library is required: importing the solver API without
+lib/libfishfry.so raises instead of falling back to anything else.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libfishfry.so")
+
+FF_OK = 0
+FF_ERR_INVALID = 1
+FF_ERR_UNSUPPORTED = 2
+FF_ERR_BYTES = 3
+FF_ERR_CUDA = 4
+FF_ERR_NOMEM = 5
+FF_ERR_TIMEOUT = 6
+FF_ERR_TASKS = 7
+
+FF_FP64 = 0
+FF_FP32 = 1
+FF_NUM_PHASES = 5
+FF_MAX_AXIS = 1800
+
+# Every symbol include/fishfry.h declares.
+EXPORTS = [
+    "ff_phase_name", "ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_destroy",
+    "ff_init_field", "ff_error_sums", "ff_modes_generate", "ff_status_string", "ff_last_error", "ff_version",
+]
+
+
+class FFError(RuntimeError):
+    """A non-zero ff_status from the C ABI; .status holds the code."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+class Mode(ctypes.Structure):
+    _fields_ = [("kx", ctypes.c_int), ("ky", ctypes.c_int), ("kz", ctypes.c_int),
+                ("a", ctypes.c_double), ("theta", ctypes.c_double)]
+
+
+class PhaseTimes(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double * FF_NUM_PHASES), ("total_ms", ctypes.c_double)]
+
+
+_lib = None
+
+
+def _declare(L):
+    i3 = ctypes.POINTER(ctypes.c_int)
+    d3 = ctypes.POINTER(ctypes.c_double)
+    vp = ctypes.c_void_p
+    L.ff_phase_name.argtypes = [ctypes.c_int]
+    L.ff_phase_name.restype = ctypes.c_char_p
+    L.ff_plan_create.argtypes = [i3, d3, d3, ctypes.c_int, ctypes.POINTER(vp)]
+    L.ff_plan_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+    L.ff_plan_info.argtypes = [vp, i3, i3]
+    L.ff_solve.argtypes = [vp, ctypes.c_size_t, vp, vp, vp, ctypes.POINTER(PhaseTimes)]
+    L.ff_plan_destroy.argtypes = [vp]
+    L.ff_init_field.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, vp]
+    L.ff_error_sums.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, d3, vp]
+    L.ff_modes_generate.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, i3, ctypes.c_double, vp]
+    L.ff_status_string.argtypes = [ctypes.c_int]
+    L.ff_status_string.restype = ctypes.c_char_p
+    L.ff_last_error.restype = ctypes.c_char_p
+    L.ff_version.restype = ctypes.c_char_p
+    for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_destroy",
+                 "ff_init_field", "ff_error_sums", "ff_modes_generate"):
+        getattr(L, name).restype = ctypes.c_int
+
+
+def lib():
+    """The loaded native library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"fishfry_b200 native library missing: {LIB_PATH} "
+                              "(build it with `python -m fishfry_b200.build`)")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def check(status, what=""):
+    if status != FF_OK:
+        L = lib()
+        raise FFError(status, f"{what}: {L.ff_status_string(status).decode()}: {L.ff_last_error().decode()}")
+
+
+def int3(v):
+    return (ctypes.c_int * 3)(*[int(x) for x in v])
+
+
+def dbl3(v):
+    return (ctypes.c_double * 3)(*[float(x) for x in v])
+
+
+def modes_array(modes):
+    """(count, void*, keepalive) for a list of (kx, ky, kz, a, theta)."""
+    if not modes:
+        return 0, None, None
+    arr = (Mode * len(modes))()
+    for q, m in enumerate(modes):
+        arr[q] = Mode(int(m[0]), int(m[1]), int(m[2]), float(m[3]), float(m[4]))
+    return len(modes), ctypes.cast(arr, ctypes.c_void_p), arr

@@ -1,0 +1,151 @@
+"""Python mirror of the reference's solver plugin and harness interface.
+
+`ParisPencil` keeps the reference constructor / bytes() / solve() contract
+(ParisPencil.hpp:23, :30, :44); `Plan` is the thinner handle over the C ABI
+with precision and stream control.  Device buffers are torch CUDA tensors (or
+raw device addresses as ints); torch is only the allocator and stream owner.
+"""
+import ctypes
+import math
+import time
+
+from . import _lib
+from ._lib import FF_FP32, FF_FP64, FF_NUM_PHASES, FFError, check, dbl3, int3, lib, modes_array
+
+
+def _ptr(buf):
+    if buf is None:
+        return None
+    if isinstance(buf, int):
+        return buf
+    return buf.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def reference_domain(n):
+    """(lo, hi, xlo, dx) the harness uses for one task: x = -pi + i*2*pi/n
+    (FishFry.hpp:109-111, :133-139)."""
+    dx = [2.0 * math.pi / n[a] if n[a] > 0 else 0.0 for a in range(3)]
+    lo = [-math.pi] * 3
+    hi = [math.pi - dx[a] for a in range(3)]
+    return lo, hi, list(lo), dx
+
+
+def phase_names():
+    return [lib().ff_phase_name(p).decode() for p in range(FF_NUM_PHASES)]
+
+
+class Plan:
+    """A planned solve of one grid: tables resident on the current device."""
+
+    def __init__(self, n, lo=None, hi=None, precision=FF_FP64):
+        n = [int(x) for x in n]
+        if lo is None:
+            lo, hi, _, _ = reference_domain(n)
+        h = ctypes.c_void_p()
+        check(lib().ff_plan_create(int3(n), dbl3(lo), dbl3(hi), int(precision), ctypes.byref(h)), "ff_plan_create")
+        self._h = h
+        self.n = tuple(n)
+        self.precision = int(precision)
+        b = ctypes.c_size_t()
+        check(lib().ff_plan_bytes(h, ctypes.byref(b)), "ff_plan_bytes")
+        self.nbytes = b.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def bytes(self):
+        return self.nbytes
+
+    def solve(self, density, potential, stream=None, nbytes=None, timed=False):
+        """Enqueue the five passes; returns per-pass ms (and waits) if timed."""
+        times = _lib.PhaseTimes() if timed else None
+        nb = self.nbytes if nbytes is None else int(nbytes)
+        check(lib().ff_solve(self._h, nb, _ptr(density), _ptr(potential), _stream(stream),
+                             ctypes.byref(times) if timed else None), "ff_solve")
+        if timed:
+            return list(times.ms), times.total_ms
+        return None
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            check(lib().ff_plan_destroy(self._h), "ff_plan_destroy")
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ParisPencil:
+    """The reference plugin interface (ParisPencil.hpp:11-59) on one GPU.
+
+    n: global points; lo/hi: physical bounds (hi one cell short of the period);
+    m: task grid, must be (1,1,1); id: task coordinates, (0,0,0).
+    """
+
+    def __init__(self, n, lo, hi, m=(1, 1, 1), id=(0, 0, 0)):
+        if tuple(m) != (1, 1, 1) or tuple(id) != (0, 0, 0):
+            raise FFError(_lib.FF_ERR_TASKS, "ParisPencil: one task on one GPU (m must be 1x1x1)")
+        self._plan = Plan(n, lo, hi, FF_FP64)
+
+    def bytes(self):
+        return self._plan.nbytes
+
+    def solve(self, bytes, density, potential, stamps):
+        """Overwrites `stamps` with [("Total", t0), (phase, t), ...]; blocks until done."""
+        stamps.clear()
+        t0 = time.monotonic()
+        stamps.append(("Total", t0))
+        ms, _ = self._plan.solve(density, potential, nbytes=bytes, timed=True)
+        t = t0
+        for name, dt in zip(phase_names(), ms):
+            t += 1e-3 * dt
+            stamps.append((name, t))
+
+
+def init_field(n, f, modes=None, precision=FF_FP64, stream=None):
+    """f on the device: analytic right-hand side (FishFry.hpp:22-44) + modes."""
+    _, _, xlo, dx = reference_domain(n)
+    nm, mp, keep = modes_array(modes)
+    check(lib().ff_init_field(int3(n), dbl3(xlo), dbl3(dx), nm, mp, int(precision), _ptr(f), _stream(stream)),
+          "ff_init_field")
+
+
+def error_sums(n, phi, modes=None, precision=FF_FP64, stream=None):
+    """{sum|d|, sum d^2, max|d|} against the analytic phi (FishFry.hpp:57-101)."""
+    _, _, xlo, dx = reference_domain(n)
+    nm, mp, keep = modes_array(modes)
+    out = (ctypes.c_double * 3)()
+    check(lib().ff_error_sums(int3(n), dbl3(xlo), dbl3(dx), nm, mp, int(precision), _ptr(phi), out,
+                              _stream(stream)), "ff_error_sums")
+    return [out[0], out[1], out[2]]
+
+
+def rel_norms(n, phi, modes=None, precision=FF_FP64, stream=None):
+    """Relative L1, L2, Linf as the harness prints them (FishFry.hpp:156-158, :198)."""
+    s = error_sums(n, None, modes, precision, stream)
+    d = error_sums(n, phi, modes, precision, stream)
+    return [d[0] / s[0], math.sqrt(d[1] / s[1]), d[2] / s[2]]
+
+
+def modes_generate(seed, count, kmax=32, kaxis=(32, 32, 32), sigma=0.1):
+    arr = (_lib.Mode * max(count, 1))()
+    check(lib().ff_modes_generate(ctypes.c_uint64(seed), int(count), int(kmax), int3(kaxis), float(sigma),
+                                  ctypes.cast(arr, ctypes.c_void_p)), "ff_modes_generate")
+    return [(m.kx, m.ky, m.kz, m.a, m.theta) for m in arr[:count]]
+
+
+def alias_free_kaxis(n, kmax=32):
+    """Largest |k_axis| kept below n_axis/2 so the analytic comparison is alias-free."""
+    return tuple(max(0, min(kmax, (int(x) - 1) // 2)) for x in n)

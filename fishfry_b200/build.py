@@ -1,0 +1,89 @@
+"""Build recipe for the fishfry_b200 native code (sm_100a only).
+
+  python -m fishfry_b200.build          # lib/libfishfry.so and bin/fishfry
+
+Everything is compiled in-tree with nvcc for `-gencode arch=compute_100a,code=sm_100a`;
+no JIT cache and no other architecture.  Rebuilds only what is out of date.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "lib", "libfishfry.so")
+BIN = os.path.join(HERE, "bin", "fishfry")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
+
+LIB_SOURCES = ["ff_solve.cu", "ff_field.cu"]
+HEADERS = ["ff_fft.cuh", "ff_status.hpp"]
+
+
+def _nvcc():
+    cand = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    return cand if os.path.exists(cand) else (shutil.which("nvcc") or "nvcc")
+
+
+def _host_cxx():
+    # the system g++ (the image also carries a wrapper that lacks some spec files)
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_lib(verbose=False, force=False):
+    srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
+    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "fishfry.h")]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    objs = []
+    for s in srcs:
+        o = os.path.join(HERE, "lib", os.path.basename(s) + ".o")
+        _run([_nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o], verbose)
+        objs.append(o)
+    tmp = LIB + ".tmp"
+    _run([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"], verbose)
+    os.replace(tmp, LIB)
+    for o in objs:
+        os.remove(o)
+    return LIB
+
+
+def build_bin(verbose=False, force=False):
+    src = os.path.join(CSRC, "main.cpp")
+    deps = [src, LIB, os.path.join(INCLUDE, "ParisPencil.hpp"), os.path.join(INCLUDE, "FishFry.hpp"),
+            os.path.join(INCLUDE, "TimeStamp.hpp"), os.path.join(INCLUDE, "fishfry.h")]
+    if not force and not _stale(BIN, deps):
+        return BIN
+    os.makedirs(os.path.dirname(BIN), exist_ok=True)
+    cuda = os.path.dirname(os.path.dirname(_nvcc()))
+    _run([_host_cxx(), "-O2", "-std=c++17", "-I" + INCLUDE, "-I" + os.path.join(cuda, "include"), src, "-o", BIN,
+          "-L" + os.path.dirname(LIB), "-lfishfry", "-Wl,-rpath,$ORIGIN/../lib",
+          "-L" + os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath," + os.path.join(cuda, "lib64")], verbose)
+    return BIN
+
+
+def build(verbose=False, force=False):
+    build_lib(verbose, force)
+    build_bin(verbose, force)
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv)

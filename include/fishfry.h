@@ -1,0 +1,127 @@
+/*
+ * fishfry_b200 C ABI -- the drop-in boundary of the B200 Poisson solve.
+ *
+ * Plain C: pointers, sizes and status codes.  No CUDA or C++ types cross this
+ * line (streams travel as void*, i.e. a cudaStream_t or NULL for the legacy
+ * default stream).  Every device pointer is caller-owned memory on the
+ * current CUDA device.
+ *
+ * Each entry point replaces one interface of the reference (trey-ornl/fishfry):
+ *   ff_plan_create   <- ParisPencil::ParisPencil(n, lo, hi, m, id)     ParisPencil.hpp:23, ParisPencil.cpp:7-82
+ *   ff_plan_bytes    <- ParisPencil::bytes()                            ParisPencil.hpp:30
+ *   ff_solve         <- ParisPencil::solve(bytes, density, potential,   ParisPencil.hpp:44, ParisPencil.cpp:95-425
+ *                        stamps)
+ *   ff_plan_destroy  <- ParisPencil::~ParisPencil()                     ParisPencil.cpp:84-93
+ *   ff_init_field    <- FishFry init kernel                             FishFry.hpp:14-45 (launch :174)
+ *   ff_error_sums    <- FishFry diff kernel + its reductions            FishFry.hpp:47-101 (launches :148, :190;
+ *                                                                       MPI_Reduce :153-154, :195-196)
+ * The C++ class in ParisPencil.hpp (same directory) wraps these with the
+ * reference's exact constructor / bytes() / solve() signatures.
+ *
+ * Errors: the reference asserts or prints and calls exit() (gpu.hpp:69-87,
+ * ParisPencil.cpp:101).  Here every entry point returns an ff_status; the
+ * message of the last failure on the calling thread is in ff_last_error().
+ */
+#ifndef FISHFRY_B200_H
+#define FISHFRY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FF_OK = 0,
+  FF_ERR_INVALID = 1,          /* bad argument (null pointer, non-positive size, ...) */
+  FF_ERR_UNSUPPORTED = 2,      /* length with a prime factor > 5, or above FF_MAX_AXIS */
+  FF_ERR_BYTES = 3,            /* caller buffers smaller than ff_plan_bytes() */
+  FF_ERR_CUDA = 4,             /* a CUDA runtime call failed (message has the name) */
+  FF_ERR_NOMEM = 5,            /* device allocation failed */
+  FF_ERR_TIMEOUT = 6,          /* a bounded device wait gave up */
+  FF_ERR_TASKS = 7             /* task grid other than 1x1x1 (single GPU only) */
+} ff_status;
+
+enum { FF_FP64 = 0, FF_FP32 = 1 };
+
+/* Longest supported axis: the shared-memory tile holds one full line per column. */
+#define FF_MAX_AXIS 1800
+
+typedef struct ff_plan ff_plan;
+
+/* One Fourier mode of the optional seeded random term of the right-hand side:
+ * f += a*cos(kx*x + ky*y + kz*z + theta), exact solution -a/|k|^2 * cos(...). */
+typedef struct {
+  int kx, ky, kz;
+  double a, theta;
+} ff_mode;
+
+/* Per-pass device times of one solve, in milliseconds (CUDA events). */
+#define FF_NUM_PHASES 5
+typedef struct {
+  double ms[FF_NUM_PHASES];
+  double total_ms;
+} ff_phase_times;
+
+/* Name of phase p (0..FF_NUM_PHASES-1), e.g. "Real-to-complex FFT in Z". */
+const char *ff_phase_name(int p);
+
+/* Plan a solve of an n[0] x n[1] x n[2] periodic grid (x slowest, z fastest:
+ * index (i*n[1]+j)*n[2]+k).  lo/hi are the physical bounds with hi one cell
+ * short of the period, as in the reference; they set the wavenumber scale
+ * dd = 2*pi*(n-1)/(n*(hi-lo)) (ParisPencil.cpp:9-11).  precision is FF_FP64
+ * (the plain method) or FF_FP32 (FP32 butterflies, FP64-generated twiddles and
+ * 1/k^2).  Allocates the plan's twiddle and index tables on the current device.
+ * Each length must be 2^a 3^b 5^c and at most FF_MAX_AXIS. */
+int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int precision, ff_plan **plan);
+
+/* Bytes each of density and potential must hold (the half spectrum
+ * n0*n1*(n2/2+1) complex values, or the real field if larger). */
+int ff_plan_bytes(const ff_plan *plan, size_t *bytes);
+
+/* Grid dimensions and precision of a plan. */
+int ff_plan_info(const ff_plan *plan, int n[3], int *precision);
+
+/* Solve lap(phi) = f.  density: device array holding f (FP64 or FP32 per the
+ * plan), at least ff_plan_bytes() bytes; it is used as a work array and
+ * destroyed.  potential: device array of the same size; receives phi in the
+ * same layout as f.  Work is enqueued on `stream` and the call returns without
+ * waiting, unless `times` is non-NULL: then it records CUDA events between the
+ * passes, waits for the stream and fills the per-pass times. */
+int ff_solve(const ff_plan *plan, size_t bytes, void *density, void *potential, void *stream,
+             ff_phase_times *times);
+
+int ff_plan_destroy(ff_plan *plan);
+
+/* Harness: write f on the device at x = xlo + i*dx (FishFry.hpp:22-44),
+ * plus sum_m a_m cos(k_m.x + theta_m) for the given modes (nmodes may be 0).
+ * precision selects a double or float field.  Enqueued on stream. */
+int ff_init_field(const int n[3], const double xlo[3], const double dx[3], int nmodes,
+                  const ff_mode *modes, int precision, void *f, void *stream);
+
+/* Harness: sums[0..2] = { sum|d|, sum d^2, max|d| } with d = phi_exact - phi
+ * (FishFry.hpp:57-101), accumulated in FP64 with a fixed-order (deterministic)
+ * two-stage reduction.  phi == NULL gives the phi = 0 pass that the reference
+ * uses for its relative-norm scales (FishFry.hpp:146-159).  sums is HOST
+ * memory; the call waits for the stream. */
+int ff_error_sums(const int n[3], const double xlo[3], const double dx[3], int nmodes,
+                  const ff_mode *modes, int precision, const void *phi, double sums[3], void *stream);
+
+/* Seeded random modes: `count` modes with integer k, 0 < |k| <= kmax and
+ * |k_axis| <= kaxis[axis]; amplitude ~ N(0, sigma), phase ~ U[0, 2*pi)
+ * (SplitMix64 counter stream + Box-Muller).  Host only. */
+int ff_modes_generate(uint64_t seed, int count, int kmax, const int kaxis[3], double sigma, ff_mode *out);
+
+/* Status text and the last error message of the calling thread. */
+const char *ff_status_string(int status);
+const char *ff_last_error(void);
+
+/* Library version string. */
+const char *ff_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,252 @@
+"""GPU parity tests of the solve through the C ABI against the CPU oracle.
+
+FP64 bar: phi within 1e-12 relative L2 of the oracle on the same f.
+FP32 bar: phi within 1e-5 relative L2 of the FP64 oracle.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FP64_TOL = 1e-12
+FP32_TOL = 1e-5
+
+
+def dev_field(torch, ff, n, modes=None, precision=0):
+    plan = ff.Plan(n, precision=precision)
+    dt = torch.float64 if precision == ff.FF_FP64 else torch.float32
+    esz = 8 if precision == ff.FF_FP64 else 4
+    count = plan.nbytes // esz
+    d = torch.empty(count, dtype=dt, device="cuda")
+    p = torch.empty(count, dtype=dt, device="cuda")
+    ff.init_field(n, d, modes, precision)
+    return plan, d, p
+
+
+def run_solve(torch, ff, n, modes=None, precision=0):
+    """(f, phi) as host arrays after one solve of the device-initialised f."""
+    plan, d, p = dev_field(torch, ff, n, modes, precision)
+    N = n[0] * n[1] * n[2]
+    f = d[:N].double().cpu().numpy().reshape(n)
+    plan.solve(d, p)
+    torch.cuda.synchronize()
+    phi = p[:N].double().cpu().numpy().reshape(n)
+    return f, phi
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+PARITY_SIZES = [(8, 8, 8), (16, 16, 16), (12, 10, 8), (5, 9, 6), (2, 3, 5), (1, 4, 6), (3, 1, 1), (1, 1, 2),
+                (30, 45, 50), (64, 48, 40), (64, 64, 64), (100, 36, 27), (96, 80, 75), (128, 128, 128),
+                (45, 81, 125), (256, 96, 72), (1800, 2, 4), (4, 1800, 6), (6, 5, 1800), (243, 16, 10)]
+
+
+@pytest.mark.parametrize("n", PARITY_SIZES)
+def test_fp64_parity_with_oracle(torch_cuda, ff, oracle, n):
+    f, phi = run_solve(torch_cuda, ff, n)
+    ref = oracle.solve(f)
+    assert rel_l2(phi, ref) <= FP64_TOL
+
+
+@pytest.mark.parametrize("n", [(16, 16, 16), (30, 45, 50), (64, 64, 64)])
+def test_fp64_parity_random_field(torch_cuda, ff, oracle, n):
+    rng = np.random.default_rng(11)
+    f = rng.standard_normal(n)
+    plan = ff.Plan(n)
+    d = torch_cuda.zeros(plan.nbytes // 8, dtype=torch_cuda.float64, device="cuda")
+    p = torch_cuda.empty_like(d)
+    N = f.size
+    d[:N] = torch_cuda.from_numpy(f.ravel()).cuda()
+    plan.solve(d, p)
+    phi = p[:N].cpu().numpy().reshape(n)
+    assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL
+
+
+def test_fp64_parity_with_modes(torch_cuda, ff, oracle):
+    n = (64, 48, 80)
+    modes = ff.modes_generate(12345, 64, 32, ff.alias_free_kaxis(n))
+    f, phi = run_solve(torch_cuda, ff, n, modes)
+    assert np.abs(f - oracle.init_f(n, modes)).max() <= 1e-13 * np.abs(f).max()
+    assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL
+    assert rel_l2(phi, oracle.phi_exact(n, modes)) <= 1e-13
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (30, 45, 50), (64, 64, 64)])
+def test_init_field_matches_oracle(torch_cuda, ff, oracle, n):
+    _, d, _ = dev_field(torch_cuda, ff, n)
+    N = n[0] * n[1] * n[2]
+    f = d[:N].cpu().numpy().reshape(n)
+    ref = oracle.init_f(n)
+    assert np.abs(f - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("n", [(8, 8, 8), (16, 16, 16)])
+def test_known_answer_norms_on_device(torch_cuda, ff, oracle, n):
+    from tests.test_oracle import KATS
+    plan, d, p = dev_field(torch_cuda, ff, n)
+    plan.solve(d, p)
+    got = ff.rel_norms(n, p)
+    for g, want in zip(got, KATS[n]):
+        assert abs(g - want) <= 1e-4 * want
+
+
+def test_error_sums_match_oracle(torch_cuda, ff, oracle):
+    n = (30, 45, 50)
+    rng = np.random.default_rng(2)
+    phi = rng.standard_normal(n)
+    t = torch_cuda.from_numpy(phi.ravel()).cuda()
+    got = ff.error_sums(n, t)
+    ref = oracle.diff_sums(phi)
+    assert np.allclose(got, ref, rtol=1e-12, atol=0)
+    z = ff.error_sums(n, None)
+    assert np.allclose(z, oracle.diff_sums(np.zeros(n)), rtol=1e-12)
+
+
+def test_solve_is_deterministic(torch_cuda, ff):
+    n = (64, 48, 40)
+    plan, d, p = dev_field(torch_cuda, ff, n)
+    N = n[0] * n[1] * n[2]
+    f0 = d.clone()
+    plan.solve(d, p)
+    a = p[:N].clone()
+    d.copy_(f0)
+    plan.solve(d, p)
+    assert torch_cuda.equal(a, p[:N])
+
+
+def test_rejects_small_buffers(torch_cuda, ff):
+    n = (16, 16, 16)
+    plan, d, p = dev_field(torch_cuda, ff, n)
+    with pytest.raises(ff.FFError) as e:
+        plan.solve(d, p, nbytes=plan.nbytes - 8)
+    assert e.value.status == ff.FF_ERR_BYTES
+
+
+def test_bytes_match_reference_formula(ff):
+    # ParisPencil.cpp:65-75 at one task: 2*ni*nj*nh doubles
+    for n in [(8, 8, 8), (30, 45, 50), (512, 512, 512), (1024, 512, 256)]:
+        plan = ff.Plan(n)
+        assert plan.nbytes == 2 * n[0] * n[1] * (n[2] // 2 + 1) * 8
+
+
+def test_paris_pencil_drop_in(torch_cuda, ff, oracle):
+    n = (32, 24, 40)
+    lo, hi, _, _ = ff.reference_domain(n)
+    pp = ff.ParisPencil(n, lo, hi, (1, 1, 1), (0, 0, 0))
+    nb = max(pp.bytes(), 8 * n[0] * n[1] * n[2])
+    d = torch_cuda.empty(nb // 8, dtype=torch_cuda.float64, device="cuda")
+    p = torch_cuda.empty_like(d)
+    ff.init_field(n, d)
+    N = n[0] * n[1] * n[2]
+    f = d[:N].cpu().numpy().reshape(n)
+    stamps = []
+    pp.solve(nb, d, p, stamps)
+    assert stamps[0][0] == "Total" and len(stamps) == 1 + ff.FF_NUM_PHASES
+    assert [s[0] for s in stamps[1:]] == ff.phase_names()
+    assert stamps[-1][1] >= stamps[0][1]
+    assert rel_l2(p[:N].cpu().numpy().reshape(n), oracle.solve(f)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 96, 80), (30, 45, 50)])
+def test_fp32_precision_form(torch_cuda, ff, oracle, n):
+    modes = ff.modes_generate(12345, 64, 32, ff.alias_free_kaxis(n))
+    f64 = oracle.init_f(n, modes)
+    ref = oracle.solve(f64)
+    plan = ff.Plan(n, precision=ff.FF_FP32)
+    d = torch_cuda.zeros(plan.nbytes // 4, dtype=torch_cuda.float32, device="cuda")
+    p = torch_cuda.empty_like(d)
+    N = f64.size
+    ff.init_field(n, d, modes, ff.FF_FP32)
+    plan.solve(d, p)
+    phi = p[:N].double().cpu().numpy().reshape(n)
+    assert rel_l2(phi, ref) <= FP32_TOL
+
+
+def test_fishfry_driver_printout(ff):
+    exe = os.path.join(ROOT, "fishfry_b200", "bin", "fishfry")
+    r = subprocess.run([exe, "1", "1", "1", "64", "64", "64", "2"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = r.stdout
+    assert re.search(r"FishFry<\w*ParisPencil>: 64x64x64 points over 1x1x1 MPI processes", out)
+    runs = re.findall(r"^(\d+): Time (\S+) Rate (\S+) L_1 (\S+) L_2 (\S+) L_\\inf (\S+)", out, re.M)
+    assert [int(r_[0]) for r_ in runs] == [0, 1, 2]
+    assert "(warmup, ignored)" in out.splitlines()[1]
+    for r_ in runs:
+        assert max(float(x) for x in r_[3:]) < 1e-14
+    assert "Times Averaged across Iterations" in out
+    for name in ["Total"] + ff.phase_names():
+        assert re.search(r"\(\s*[\d.]+%\) \| " + re.escape(name) + "$", out, re.M)
+
+
+def test_fishfry_driver_known_answer(ff):
+    from tests.test_oracle import KATS
+    exe = os.path.join(ROOT, "fishfry_b200", "bin", "fishfry")
+    r = subprocess.run([exe, "1", "1", "1", "16", "16", "16"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    m = re.search(r"L_1 (\S+) L_2 (\S+) L_\\inf (\S+)", r.stdout)
+    for g, want in zip(map(float, m.groups()), KATS[(16, 16, 16)]):
+        assert abs(g - want) <= 1e-4 * want
+
+
+# ------------------------------------------------------- full-size workloads
+@pytest.mark.slow
+@pytest.mark.parametrize("n", [(512, 512, 512), (1024, 512, 256)])
+def test_full_size_fp64(torch_cuda, ff, oracle, n):
+    """Size-independent properties at the headline sizes: analytic error at
+    round-off, and parity with the oracle (OpenMP) on the same f."""
+    plan, d, p = dev_field(torch_cuda, ff, n)
+    N = n[0] * n[1] * n[2]
+    f = d[:N].cpu().numpy().reshape(n)
+    plan.solve(d, p)
+    assert max(ff.rel_norms(n, p)) < 1e-13
+    phi = p[:N].cpu().numpy().reshape(n)
+    del d, p
+    assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL
+
+
+@pytest.mark.slow
+def test_full_size_fp32_1024(torch_cuda, ff):
+    """1024^3 FP32 precision form with 64 random modes: relative L2 against the
+    analytic solution (the oracle is too slow at this size; the analytic phi
+    is exact to round-off for the alias-free modes)."""
+    n = (1024, 1024, 1024)
+    modes = ff.modes_generate(12345, 64, 32, ff.alias_free_kaxis(n))
+    plan = ff.Plan(n, precision=ff.FF_FP32)
+    d = torch_cuda.empty(plan.nbytes // 4, dtype=torch_cuda.float32, device="cuda")
+    p = torch_cuda.empty_like(d)
+    ff.init_field(n, d, modes, ff.FF_FP32)
+    plan.solve(d, p)
+    s0 = ff.error_sums(n, None, modes, ff.FF_FP32)
+    s1 = ff.error_sums(n, p, modes, ff.FF_FP32)
+    assert (s1[1] / s0[1]) ** 0.5 <= FP32_TOL
+
+
+# ----------------------------------------- the reference itself (oracle/_ref)
+REF_DUMP = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_DUMP), reason="reference not built (oracle/ref/Makefile)")
+@pytest.mark.parametrize("n", [(8, 8, 8), (12, 10, 8), (30, 45, 50), (64, 64, 64), (100, 36, 27)])
+def test_parity_with_reference_binary(torch_cuda, ff, n, tmp_path):
+    out = tmp_path / "ref.bin"
+    r = subprocess.run([REF_DUMP, str(n[0]), str(n[1]), str(n[2]), str(out)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    raw = np.fromfile(out, dtype=np.uint8)
+    N = n[0] * n[1] * n[2]
+    arr = raw[12:].view(np.float64)
+    f_ref, phi_ref = arr[:N].reshape(n), arr[N:].reshape(n)
+    plan = ff.Plan(n)
+    d = torch_cuda.zeros(plan.nbytes // 8, dtype=torch_cuda.float64, device="cuda")
+    p = torch_cuda.empty_like(d)
+    d[:N] = torch_cuda.from_numpy(f_ref.ravel()).cuda()
+    plan.solve(d, p)
+    phi = p[:N].cpu().numpy().reshape(n)
+    assert rel_l2(phi, phi_ref) <= FP64_TOL
