@@ -25,7 +25,7 @@ FF_MAX_AXIS = 1800
 
 # Every symbol include/fishfry.h declares.
 EXPORTS = [
-    "ff_phase_name", "ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_destroy",
+    "ff_phase_name", "ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
     "ff_init_field", "ff_error_sums", "ff_modes_generate", "ff_status_string", "ff_last_error", "ff_version",
 ]
 
@@ -60,6 +60,7 @@ def _declare(L):
     L.ff_plan_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.ff_plan_info.argtypes = [vp, i3, i3]
     L.ff_solve.argtypes = [vp, ctypes.c_size_t, vp, vp, vp, ctypes.POINTER(PhaseTimes)]
+    L.ff_plan_check.argtypes = [vp, vp]
     L.ff_plan_destroy.argtypes = [vp]
     L.ff_init_field.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, vp]
     L.ff_error_sums.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, d3, vp]
@@ -68,7 +69,7 @@ def _declare(L):
     L.ff_status_string.restype = ctypes.c_char_p
     L.ff_last_error.restype = ctypes.c_char_p
     L.ff_version.restype = ctypes.c_char_p
-    for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_destroy",
+    for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
                  "ff_init_field", "ff_error_sums", "ff_modes_generate"):
         getattr(L, name).restype = ctypes.c_int
 

@@ -75,6 +75,10 @@ class Plan:
             return list(times.ms), times.total_ms
         return None
 
+    def check(self, stream=None):
+        """Raises FFError(FF_ERR_TIMEOUT) if a kernel's bounded wait gave up."""
+        check(lib().ff_plan_check(self._h, _stream(stream)), "ff_plan_check")
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             check(lib().ff_plan_destroy(self._h), "ff_plan_destroy")

@@ -1,10 +1,15 @@
 // Shared-memory batched FFT engine for sm_100a.
 //
-// A thread block owns a tile of W independent lines ("columns") of length n.
-// The tile lives in shared memory point-major: element (pos, c) at
-// sm[pos*W + c], so that one row of W complex values is exactly 128 bytes
-// (W = 8 for FP64, 16 for FP32).  A warp always touches whole rows, which
-// keeps every shared-memory access conflict-free for any stage stride.
+// A thread block transforms a tile of W independent lines ("columns") of
+// length n held in shared memory.  Two tile layouts are used:
+//   * point-major  sm[pos*W + c]: one row of W complex values is 128 bytes
+//     (W = 8 FP64 / 16 FP32); threads take columns fastest, so a warp always
+//     touches whole rows and every access is bank-conflict free.  Used by the
+//     strided passes (y and x), whose global rows are W contiguous columns.
+//   * line-major   sm[c*P + swz(pos)]: each line contiguous (pitch P), with an
+//     XOR swizzle of the 16-byte chunk inside every 128-byte row so unit-,
+//     8- and 64-element strides are all conflict free.  Used by the z passes,
+//     whose global lines are contiguous; threads take positions fastest.
 //
 // Transforms are in-place mixed-radix Cooley-Tukey:
 //   * decimation in frequency (DIF): natural input, output at position pos
@@ -12,9 +17,9 @@
 //   * decimation in time (DIT): the transpose, digit-reversed input, natural
 //     output.
 // Stage s (radix R, span L) works on groups {blk*L + j + r*(L/R)}, r < R.
-// The first stage may read straight from global memory and the last stage may
-// write straight to global memory (loader / storer functors), so a pass moves
-// each element between HBM and the SM once.
+// Loads and stores of a stage go through accessor functors, so the first
+// stage can read global memory (or another buffer) and the last can write
+// global memory (or another buffer) directly.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -23,14 +28,10 @@
 namespace ff {
 
 constexpr int kMaxStages = 16;
-constexpr int kThreads = 256;
 
 template <typename T> struct Cplx;
 template <> struct Cplx<double> { using type = double2; };
 template <> struct Cplx<float> { using type = float2; };
-
-// Columns per tile: one 128-byte shared-memory row.
-template <typename T> struct TileW { static constexpr int value = 128 / (2 * sizeof(T)); };
 
 __device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
 __device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
@@ -154,32 +155,114 @@ template <bool INV, typename C> struct Dft<8, INV, C> {
   }
 };
 
+// ------------------------------------------------------------ radix plan
+// Radix order of a DIF transform of length n = 2^a 3^b 5^c: radix 8 while
+// three factors of 2 remain, then one 4 or 2, then the 5s, then the 3s; a
+// length of 1 is one stage of radix 1.  Shared by host planning and device
+// code, so compile-time specialised kernels and plan tables agree.
+__host__ __device__ constexpr int plan_radix(int n, int s) {
+  int twos = 0, fives = 0, threes = 0, m = n;
+  while (m > 1 && m % 2 == 0) { m /= 2; twos++; }
+  while (m > 1 && m % 5 == 0) { m /= 5; fives++; }
+  while (m > 1 && m % 3 == 0) { m /= 3; threes++; }
+  const int eights = twos / 3, rest = twos % 3;
+  if (s < eights) return 8;
+  s -= eights;
+  if (rest) {
+    if (s == 0) return rest == 2 ? 4 : 2;
+    s -= 1;
+  }
+  if (s < fives) return 5;
+  s -= fives;
+  if (s < threes) return 3;
+  return 1;
+}
+__host__ __device__ constexpr int plan_stages(int n) {
+  int s = 0;
+  for (int q = 0, L = n; L > 1; q++) {
+    const int r = plan_radix(n, q);
+    if (r == 1) break;   // n is not 2^a 3^b 5^c
+    L /= r;
+    s++;
+  }
+  return s > 0 ? s : 1;
+}
+// Span (sub-transform length) of stage s.
+__host__ __device__ constexpr int plan_span(int n, int s) {
+  int L = n;
+  for (int q = 0; q < s; q++) L /= plan_radix(n, q);
+  return L;
+}
+
 // One axis of a plan as the kernels see it.
 template <typename C> struct AxisDev {
   int n;
   int nstages;
   int radix[kMaxStages];   // DIF order: stage 0 spans the whole line
-  const C *tw;             // tw[q] = exp(-2*pi*i*q/n), q < n (FP64-generated)
+  const C *tw;             // tw[q] = exp(-2*pi*i*q/n), q < n (FP64-generated, in C's precision)
+  const double2 *tw64;     // the same table in FP64
   const int *rev;          // DIF output position -> frequency index
   const int *ipos;         // frequency index -> DIF output position
 };
+
+__device__ __forceinline__ double2 to_c(double2 w, double2 *) { return w; }
+__device__ __forceinline__ float2 to_c(double2 w, float2 *) { return make_float2((float)w.x, (float)w.y); }
 
 template <bool INV, typename C> __device__ __forceinline__ C twmul(C v, const C *__restrict__ tw, int q) {
   const C w = __ldg(tw + q);
   return INV ? cmulc(v, w) : cmul(v, w);
 }
 
+// v[r] *= w^(+-j*r) for r = 1..R-1 with w = exp(-2*pi*i*twstep/n).
+//   TWREC = false: one table load per factor (the loads are shared by the
+//                  threads of a warp that hold the same j);
+//   TWREC = true:  one FP64 table load, the powers by FP64 complex products
+//                  (for thread orders in which every lane has its own j).
+template <int R, bool INV, bool TWREC, typename C>
+__device__ __forceinline__ void apply_twiddles(C *v, int j, int twstep, const C *__restrict__ tw,
+                                               const double2 *__restrict__ tw64) {
+  if (TWREC) {
+    double2 w1 = __ldg(tw64 + j * twstep);
+    if (INV) w1.y = -w1.y;
+    double2 w = w1;
+#pragma unroll
+    for (int r = 1; r < R; r++) {
+      v[r] = cmul(v[r], to_c(w, (C *)nullptr));
+      if (r + 1 < R) w = cmul(w, w1);
+    }
+  } else {
+#pragma unroll
+    for (int r = 1; r < R; r++) v[r] = twmul<INV>(v[r], tw, j * r * twstep);
+  }
+}
+
+// Thread-to-item order of a stage: columns fastest (point-major tiles) or
+// butterflies fastest (line-major tiles).
+enum class Map { ColFast, PosFast };
+
 // One stage over all (group, column) items of the tile.
 //   DIT = false: DFT then output twiddles (DIF);  DIT = true: input twiddles then DFT.
 //   ld(pos, c) -> C,  st(pos, c, C).
-template <int R, bool INV, bool DIT, int W, typename C, typename LD, typename ST>
-__device__ __forceinline__ void run_stage(int n, int L, const C *__restrict__ tw, LD &ld, ST &st) {
+//   ncols: columns in the tile (must be W for Map::ColFast).
+//   NC, LC > 0: compile-time length and span (NC = 0: use n_rt, L_rt);
+//   NT > 0: compile-time block size; with NC it fully unrolls the item loop.
+template <int R, bool INV, bool DIT, Map MAP, int W, int NT, int NC, int LC, bool TWREC, typename C, typename LD,
+          typename ST>
+__device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, LD &ld, ST &st, int ncols) {
+  const int n = NC ? NC : n_rt;
+  const int L = NC ? LC : L_rt;
   const int m = L / R;
   const int twstep = n / L;
-  const int items = W * (n / R);
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {
-    const int c = it % W;
-    const int b = it / W;
+  const int nb = n / R;
+  auto body = [&](int it) {
+    int c, b;
+    if (MAP == Map::ColFast) {
+      c = it % W;
+      b = it / W;
+    } else {
+      b = it % nb;
+      c = it / nb;
+    }
     const int blk = b / m;
     const int j = b - blk * m;
     const int base = blk * L + j;
@@ -187,20 +270,23 @@ __device__ __forceinline__ void run_stage(int n, int L, const C *__restrict__ tw
 #pragma unroll
     for (int r = 0; r < R; r++) v[r] = ld(base + r * m, c);
     if (DIT) {
-      if (j != 0) {
-#pragma unroll
-        for (int r = 1; r < R; r++) v[r] = twmul<INV>(v[r], tw, j * r * twstep);
-      }
+      if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
       Dft<R, INV, C>::run(v);
     } else {
       Dft<R, INV, C>::run(v);
-      if (j != 0) {
-#pragma unroll
-        for (int r = 1; r < R; r++) v[r] = twmul<INV>(v[r], tw, j * r * twstep);
-      }
+      if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
     }
 #pragma unroll
     for (int r = 0; r < R; r++) st(base + r * m, c, v[r]);
+  };
+  if constexpr (NC > 0 && NT > 0 && MAP == Map::ColFast && (W * (NC / R)) % NT == 0) {
+    constexpr int ITER = W * (NC / R) / NT;
+#pragma unroll
+    for (int q = 0; q < ITER; q++) body((int)threadIdx.x + q * NT);
+  } else {
+    const int items = ncols * nb;
+    const int step = NT > 0 ? NT : (int)blockDim.x;
+    for (int it = threadIdx.x; it < items; it += step) body(it);
   }
 }
 
@@ -217,55 +303,199 @@ template <typename F> __device__ __forceinline__ void with_radix(int r, F &&f) {
   }
 }
 
-// Shared-memory accessors of the point-major tile.
-template <int W, typename C> struct SmemLd {
-  const C *sm;
-  __device__ __forceinline__ C operator()(int pos, int c) const { return sm[pos * W + c]; }
-};
-template <int W, typename C> struct SmemSt {
+// ------------------------------------------------------------ accessors
+// Point-major tile: element (pos, c) at sm[pos*W + c].
+template <int W, typename C> struct PointTile {
   C *sm;
+  __device__ __forceinline__ C operator()(int pos, int c) const { return sm[pos * W + c]; }
   __device__ __forceinline__ void operator()(int pos, int c, C v) const { sm[pos * W + c] = v; }
 };
 
-// Full DIF transform of the tile: stage 0 reads through ldg, the last stage
-// writes through stg, the stages in between work in shared memory.  Ends with
-// a block barrier.
-template <bool INV, int W, typename C, typename LDG, typename STG>
-__device__ __forceinline__ void dif_transform(const AxisDev<C> &ax, C *sm, LDG &ldg, STG &stg) {
-  SmemLd<W, C> sld{sm};
-  SmemSt<W, C> sst{sm};
+// Line-major swizzled tile: element (pos, c) at sm[c*P + swz(pos)]; the 16-byte
+// chunk index inside each 128-byte row is XORed with the row index mod 8.
+// P must be a multiple of 8 (FP64) or 16 (FP32) elements.
+__device__ __forceinline__ int swz(int pos, double2 *) { return pos ^ ((pos >> 3) & 7); }
+__device__ __forceinline__ int swz(int pos, float2 *) { return pos ^ (((pos >> 4) & 7) << 1); }
+
+template <typename C> struct LineTile {
+  C *sm;
+  int P;
+  __device__ __forceinline__ int at(int pos, int c) const { return c * P + swz(pos, (C *)nullptr); }
+  __device__ __forceinline__ C operator()(int pos, int c) const { return sm[at(pos, c)]; }
+  __device__ __forceinline__ void operator()(int pos, int c, C v) const { sm[at(pos, c)] = v; }
+};
+
+// Digit reversal of a compile-time plan: the frequency held at DIF output
+// position pos (the host builds the same table for runtime plans).
+template <int N> __device__ __forceinline__ int rev_ct(int pos) {
+  int k = 0, kmul = 1, span = N;
+#pragma unroll
+  for (int s = 0; s < plan_stages(N); s++) {
+    const int r = plan_radix(N, s);
+    span /= r;
+    const int m = pos / span;
+    pos -= m * span;
+    k += m * kmul;
+    kmul *= r;
+  }
+  return k;
+}
+
+// Frequency index of a position written by the LAST DIF stage (span R):
+// rev[base + r] = rev[base] + r*(n/R), so one table load serves the group.
+// RC, NRC > 0: compile-time R and n/R.
+template <int RC = 0, int NRC = 0> struct RevLast {
+  const int *rev;
+  int R, nR;
+  __device__ __forceinline__ int operator()(int pos) const {
+    const int Rv = RC ? RC : R;
+    const int r = pos % Rv;
+    return __ldg(rev + pos - r) + r * (NRC ? NRC : nR);
+  }
+};
+
+template <int N> struct RevCT {
+  __device__ __forceinline__ int operator()(int pos) const { return rev_ct<N>(pos); }
+};
+
+// Line-major tile written at the natural (frequency) index of a DIF output
+// position: the out-of-place last stage of a DIF transform.
+template <typename C, typename RL> struct LineTileRev {
+  LineTile<C> t;
+  RL rl;
+  __device__ __forceinline__ void operator()(int pos, int c, C v) const { t(rl(pos), c, v); }
+};
+
+// ------------------------------------------------------------ stage drivers
+// Runtime plan.  DIF stages 0..S-1: stage 0 reads ld0 (with recurrence
+// twiddles if TWREC0), stage S-1 writes stl, the others read and write mid.
+// A block barrier follows every stage.
+template <bool INV, Map MAP, int W, int NT, bool TWREC0, typename C, typename LD0, typename MID, typename STL>
+__device__ __forceinline__ void dif_rt(const AxisDev<C> &ax, int S, LD0 &ld0, MID &mid, STL &stl, int ncols) {
   int L = ax.n;
-  for (int s = 0; s < ax.nstages; s++) {
-    const bool first = s == 0, last = s == ax.nstages - 1;
+  for (int s = 0; s < S; s++) {
     with_radix(ax.radix[s], [&](auto tag) {
       constexpr int R = decltype(tag)::value;
-      if (first && last) run_stage<R, INV, false, W>(ax.n, L, ax.tw, ldg, stg);
-      else if (first) run_stage<R, INV, false, W>(ax.n, L, ax.tw, ldg, sst);
-      else if (last) run_stage<R, INV, false, W>(ax.n, L, ax.tw, sld, stg);
-      else run_stage<R, INV, false, W>(ax.n, L, ax.tw, sld, sst);
+      if (s == 0 && s == S - 1) stage<R, INV, false, MAP, W, NT, 0, 0, TWREC0>(ax.n, L, ax, ld0, stl, ncols);
+      else if (s == 0) stage<R, INV, false, MAP, W, NT, 0, 0, TWREC0>(ax.n, L, ax, ld0, mid, ncols);
+      else if (s == S - 1) stage<R, INV, false, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, stl, ncols);
+      else stage<R, INV, false, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, mid, ncols);
     });
     L /= ax.radix[s];
     __syncthreads();
   }
 }
 
-// DIT stages nstages-1 .. s_end (inclusive) on a digit-reversed tile already in
-// shared memory; stage 0 (if s_end == 0) writes through stg.  Ends with a barrier.
-template <bool INV, int W, typename C, typename STG>
-__device__ __forceinline__ void dit_stages(const AxisDev<C> &ax, C *sm, int s_begin, STG &stg) {
-  SmemLd<W, C> sld{sm};
-  SmemSt<W, C> sst{sm};
-  // span of stage s is n / (r_0 ... r_{s-1})
+// Runtime plan.  DIT stages s_begin..0 on a digit-reversed tile in mid;
+// stage 0 writes stl.  A block barrier follows every stage.
+template <bool INV, Map MAP, int W, int NT, typename C, typename MID, typename STL>
+__device__ __forceinline__ void dit_rt(const AxisDev<C> &ax, int s_begin, MID &mid, STL &stl, int ncols) {
   for (int s = s_begin; s >= 0; s--) {
     int L = ax.n;
     for (int q = 0; q < s; q++) L /= ax.radix[q];
     with_radix(ax.radix[s], [&](auto tag) {
       constexpr int R = decltype(tag)::value;
-      if (s == 0) run_stage<R, INV, true, W>(ax.n, L, ax.tw, sld, stg);
-      else run_stage<R, INV, true, W>(ax.n, L, ax.tw, sld, sst);
+      if (s == 0) stage<R, INV, true, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, stl, ncols);
+      else stage<R, INV, true, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, mid, ncols);
     });
     __syncthreads();
   }
 }
+
+// Compile-time plan of length N: DIF stages s..SEND-1 as dif_rt does.
+// TWREC0: recurrence twiddles in stage 0; TWALL: in every stage.
+template <int N, int SEND, int s, bool INV, Map MAP, int W, int NT, bool TWREC0, bool TWALL, typename C,
+          typename LD0, typename MID, typename STL>
+__device__ __forceinline__ void dif_ct(const AxisDev<C> &ax, LD0 &ld0, MID &mid, STL &stl, int ncols) {
+  if constexpr (s < SEND) {
+    constexpr int R = plan_radix(N, s);
+    constexpr int L = plan_span(N, s);
+    constexpr bool TWR = TWALL || (TWREC0 && s == 0);
+    if constexpr (s == 0 && SEND == 1) stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, ld0, stl, ncols);
+    else if constexpr (s == 0) stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, ld0, mid, ncols);
+    else if constexpr (s == SEND - 1) stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, mid, stl, ncols);
+    else stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, mid, mid, ncols);
+    __syncthreads();
+    dif_ct<N, SEND, s + 1, INV, MAP, W, NT, TWREC0, TWALL>(ax, ld0, mid, stl, ncols);
+  }
+}
+
+// Compile-time plan of length N: DIT stages s..0 as dit_rt does.
+template <int N, int s, bool INV, Map MAP, int W, int NT, bool TWALL, typename C, typename MID, typename STL>
+__device__ __forceinline__ void dit_ct(const AxisDev<C> &ax, MID &mid, STL &stl, int ncols) {
+  if constexpr (s >= 0) {
+    constexpr int R = plan_radix(N, s);
+    constexpr int L = plan_span(N, s);
+    if constexpr (s == 0) stage<R, INV, true, MAP, W, NT, N, L, TWALL>(N, L, ax, mid, stl, ncols);
+    else stage<R, INV, true, MAP, W, NT, N, L, TWALL>(N, L, ax, mid, mid, ncols);
+    __syncthreads();
+    dit_ct<N, s - 1, INV, MAP, W, NT, TWALL>(ax, mid, stl, ncols);
+  }
+}
+
+// Full DIF transform (all stages) with a compile-time (N > 0) or runtime plan.
+template <int N, bool INV, Map MAP, int W, int NT, bool TWREC0, bool TWALL, typename C, typename LD0, typename MID,
+          typename STL>
+__device__ __forceinline__ void dif_all(const AxisDev<C> &ax, LD0 &ld0, MID &mid, STL &stl, int ncols) {
+  if constexpr (N > 0) dif_ct<N, plan_stages(N), 0, INV, MAP, W, NT, TWREC0, TWALL>(ax, ld0, mid, stl, ncols);
+  else dif_rt<INV, MAP, W, NT, TWREC0>(ax, ax.nstages, ld0, mid, stl, ncols);
+}
+
+// ------------------------------------------------ TMA and mbarrier helpers
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *m, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's earlier generic-proxy shared-memory accesses before
+// later async-proxy (TMA) accesses of the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *m, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for phase `parity` of m with an iteration limit (about a second with
+// the back-off); returns false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *m, uint32_t parity) {
+  for (int i = 0; i < (1 << 24); i++) {
+    if (mbar_try_wait(m, parity)) return true;
+    if (i >= 32) __nanosleep(64);
+  }
+  return false;
+}
+
+// 3-D tiled TMA load of one box into shared memory, completing on m.
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int x, int y, int z, uint64_t *m) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(m))
+      : "memory");
+}
+
+// Device-side status word values (plan status buffer).
+enum : int { kDevOk = 0, kDevTmaTimeout = 1 };
 
 }  // namespace ff

@@ -17,6 +17,7 @@
 // The reference's 12 reorder kernels and 6 MPI_Alltoall self-copies reduce to
 // the choice of row stride in passes 2-4.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,21 +37,46 @@ template <typename T> struct PassArgs {
   AxisDev<C> ax[3];        // 0: x (n = ni), 1: y (nj), 2: z (nk)
   const double *kk[3];     // (min(i, n-i) * dd)^2 per axis; kk[2] indexed by kh
   double invN;             // 1 / (ni*nj*nk)
+  double dd[3];            // wavenumber scales (ParisPencil.cpp:9-11)
+  int *status;             // device status word (kDev*), 0 = ok
 };
 
+constexpr int kZThreads = 256;
+
+// Lengths with compile-time specialised kernels (fully unrolled stages);
+// every other length runs the same kernels with the plan read at run time.
+#define FF_FOR_EACH_SPECIAL_N(X) X(256) X(512) X(1024)
+
+// Frequency of a last-stage DIF position: arithmetic for compile-time plans,
+// one table load per radix group otherwise.
+template <int N> struct RevLastOf { using type = RevCT<N>; };
+template <> struct RevLastOf<0> { using type = RevLast<0, 0>; };
+template <int N, typename C> __device__ __forceinline__ typename RevLastOf<N>::type rev_last(const AxisDev<C> &ax) {
+  if constexpr (N > 0) {
+    return RevCT<N>{};
+  } else {
+    const int R = ax.radix[ax.nstages - 1];
+    return RevLast<0, 0>{ax.rev, R, ax.n / R};
+  }
+}
+
 // ------------------------------------------------------------------ pass 1
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_zfwd(const T *__restrict__ f, typename Cplx<T>::type *__restrict__ spec,
-                                                   const PassArgs<T> a) {
+// Tile: W line pairs (2W consecutive real lines), two line-major buffers A, B
+// of pitch P.  Line pair c is transformed as z = f[line a] + i f[line b].
+template <typename T, int N>
+__global__ void __launch_bounds__(kZThreads) k_zfwd(const T *__restrict__ f, typename Cplx<T>::type *__restrict__ spec,
+                                                    const PassArgs<T> a, int W, int P) {
   using C = typename Cplx<T>::type;
-  constexpr int W = TileW<T>::value;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C *sm = reinterpret_cast<C *>(smraw);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  C *A = reinterpret_cast<C *>(smraw);
+  C *B = A + W * P;
   const long nlines = (long)a.ni * a.nj;
   const long line0 = (long)blockIdx.x * (2 * W);
-  const int nk = a.nk;
+  const int nk = N > 0 ? N : a.nk;
+  const AxisDev<C> &ax = a.ax[2];
 
-  // element pos of pair c: z = f[line a] + i f[line b]
+  // stage 0 reads the two real lines straight from HBM, consecutive threads on
+  // consecutive points of one line
   auto ldg = [&](int pos, int c) -> C {
     const long la = line0 + 2 * c;
     T x = 0, y = 0;
@@ -58,54 +84,83 @@ __global__ void __launch_bounds__(kThreads) k_zfwd(const T *__restrict__ f, type
     if (la + 1 < nlines) y = f[(la + 1) * nk + pos];
     return mk(x, y);
   };
-  SmemSt<W, C> sst{sm};
-  dif_transform<false, W>(a.ax[2], sm, ldg, sst);
+  LineTile<C> tA{A, P}, tB{B, P};
+  LineTileRev<C, typename RevLastOf<N>::type> tBrev{tB, rev_last<N>(ax)};
+  dif_all<N, false, Map::PosFast, 1, kZThreads, true, false>(ax, ldg, tA, tBrev, W);   // B: Z in natural order
 
   // split: A[k] = (Z[k] + conj Z[n-k]) / 2,  B[k] = (Z[k] - conj Z[n-k]) / (2i)
-  const int *ipos = a.ax[2].ipos;
   const T h = (T)0.5;
-  for (int it = threadIdx.x; it < W * a.nh; it += blockDim.x) {
-    const int c = it % W;
-    const int k = it / W;
+  const int nh = a.nh;
+  for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+    const int k = it % nh;
+    const int c = it / nh;
     const long la = line0 + 2 * c;
     if (la >= nlines) continue;
-    const C z = sm[__ldg(ipos + k) * W + c];
-    const C w = sm[__ldg(ipos + (k == 0 ? 0 : nk - k)) * W + c];
+    const C z = tB(k, c);
+    const C w = tB(k == 0 ? 0 : nk - k, c);
     spec[la * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
     if (la + 1 < nlines) spec[(la + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
   }
 }
 
-// ------------------------------------------------------------- passes 2, 4
-// Complex transform along y of tile (i = blockIdx.y, kh0 = blockIdx.x*W).
-template <typename T, bool INV>
-__global__ void __launch_bounds__(kThreads) k_ypass(const typename Cplx<T>::type *src, typename Cplx<T>::type *dst,
-                                                    const PassArgs<T> a) {
+// ------------------------------------------------------------------ pass 5
+template <typename T, int N>
+__global__ void __launch_bounds__(kZThreads) k_zinv(const typename Cplx<T>::type *__restrict__ spec, T *__restrict__ out,
+                                                    const PassArgs<T> a, int W, int P) {
   using C = typename Cplx<T>::type;
-  constexpr int W = TileW<T>::value;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C *sm = reinterpret_cast<C *>(smraw);
-  const int kh0 = blockIdx.x * W;
-  const int ncol = min(W, a.nh - kh0);
-  const long base = (long)blockIdx.y * a.nj * a.nhp + kh0;
-  const int pitch = a.nhp;
-  const int *rev = a.ax[1].rev;
-  auto ldg = [&](int pos, int c) -> C { return c < ncol ? src[base + (long)pos * pitch + c] : mk((T)0, (T)0); };
-  auto stg = [&](int pos, int c, C v) {
-    if (c < ncol) dst[base + (long)__ldg(rev + pos) * pitch + c] = v;
-  };
-  dif_transform<INV, W>(a.ax[1], sm, ldg, stg);
+  extern __shared__ __align__(128) unsigned char smraw[];
+  C *A = reinterpret_cast<C *>(smraw);
+  C *B = A + W * P;
+  const long nlines = (long)a.ni * a.nj;
+  const long line0 = (long)blockIdx.x * (2 * W);
+  const int nk = N > 0 ? N : a.nk;
+  const int nh = a.nh;
+  const AxisDev<C> &ax = a.ax[2];
+  LineTile<C> tA{A, P}, tB{B, P};
+  LineTileRev<C, typename RevLastOf<N>::type> tBrev{tB, rev_last<N>(ax)};
+
+  // Z[k] = A[k] + i B[k] over the Hermitian extension, natural order in B; the
+  // imaginary parts of the zero and Nyquist terms are dropped, as a C2R
+  // transform does.
+  for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+    const int k = it % nh;
+    const int c = it / nh;
+    const long la = line0 + 2 * c;
+    C sa = mk((T)0, (T)0), sb = mk((T)0, (T)0);
+    if (la < nlines) sa = spec[la * a.nhp + k];
+    if (la + 1 < nlines) sb = spec[(la + 1) * a.nhp + k];
+    if (k == 0 || 2 * k == nk) {
+      tB(k, c, mk(sa.x, sb.x));
+    } else {
+      tB(k, c, mk(sa.x - sb.y, sa.y + sb.x));
+      tB(nk - k, c, mk(sa.x + sb.y, sb.x - sa.y));
+    }
+  }
+  __syncthreads();
+  dif_all<N, true, Map::PosFast, 1, kZThreads, true, false>(ax, tB, tA, tBrev, W);   // B: z in natural order
+
+  for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
+    const int t = it % nk;
+    const int c = it / nk;
+    const long la = line0 + 2 * c;
+    const C v = tB(t, c);
+    if (la < nlines) out[la * nk + t] = v.x;
+    if (la + 1 < nlines) out[(la + 1) * nk + t] = v.y;
+  }
 }
 
-// ------------------------------------------------------------------ pass 3
-// Forward transform along x, filter, inverse transform along x, for tile
-// (j = blockIdx.y, kh0 = blockIdx.x*W).  DIF forward leaves the spectrum
-// digit-reversed in shared memory; the last DIF stage, the filter and the first
+// ------------------------------------------------------------- passes 2-4
+// Persistent strided pass.  A tile is W consecutive kh columns of all n rows
+// of one plane (y pass: fixed i, rows j; x pass: fixed j, rows i), held
+// point-major and brought in by TMA; results leave from registers straight
+// to HBM in the last stage.
+//
+// The last DIF stage of the x forward transform, the filter and the first
 // DIT stage of the inverse act on the same register group.
-template <int R, int W, typename C, typename LD, typename ST, typename FL>
-__device__ __forceinline__ void fused_filter_stage(int n, LD &ld, ST &st, FL &filt) {
-  const int items = W * (n / R);
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {
+template <int R, int W, int NT, int NC, typename C, typename LD, typename ST, typename FL>
+__device__ __forceinline__ void fused_filter_stage(int n_rt, LD &ld, ST &st, FL &filt) {
+  const int n = NC ? NC : n_rt;
+  auto body = [&](int it) {
     const int c = it % W;
     const int base = (it / W) * R;
     C v[R];
@@ -117,100 +172,121 @@ __device__ __forceinline__ void fused_filter_stage(int n, LD &ld, ST &st, FL &fi
     Dft<R, true, C>::run(v);
 #pragma unroll
     for (int r = 0; r < R; r++) st(base + r, c, v[r]);
+  };
+  if constexpr (NC > 0 && (W * (NC / R)) % NT == 0) {
+    constexpr int ITER = W * (NC / R) / NT;
+#pragma unroll
+    for (int q = 0; q < ITER; q++) body((int)threadIdx.x + q * NT);
+  } else {
+    for (int it = threadIdx.x; it < W * (n / R); it += NT) body(it);
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_xpass(typename Cplx<T>::type *data, const PassArgs<T> a) {
-  using C = typename Cplx<T>::type;
-  constexpr int W = TileW<T>::value;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C *sm = reinterpret_cast<C *>(smraw);
-  const int j = blockIdx.y;
-  const int kh0 = blockIdx.x * W;
-  const int ncol = min(W, a.nh - kh0);
-  const long base = (long)j * a.nhp + kh0;
-  const long pitch = (long)a.nj * a.nhp;
-  const AxisDev<C> &ax = a.ax[0];
-  const int n = ax.n;
-  const int S = ax.nstages;
-
-  auto ldg = [&](int pos, int c) -> C { return c < ncol ? data[base + pos * pitch + c] : mk((T)0, (T)0); };
-  auto stg = [&](int pos, int c, C v) {
-    if (c < ncol) data[base + pos * pitch + c] = v;
-  };
-  const double j2 = __ldg(a.kk[1] + j);
-  const double *kkx = a.kk[0];
-  const double *kkz = a.kk[2];
-  const int *rev = ax.rev;
-  const double invN = a.invN;
-  // d = -1/((i2 + j2) + k2) as ParisPencil.cpp:276-279 forms it, times 1/N
-  auto filt = [&](int pos, int c, C v) -> C {
-    const int kx = __ldg(rev + pos);
-    const int kh = kh0 + c;
-    if (c >= ncol) return v;
-    if ((kx | j | kh) == 0) return mk((T)0, (T)0);
-    const double d = -1.0 / ((__ldg(kkx + kx) + j2) + __ldg(kkz + kh)) * invN;
-    return cscale(v, (T)d);
-  };
-
-  SmemLd<W, C> sld{sm};
-  SmemSt<W, C> sst{sm};
-  int L = n;
-  for (int s = 0; s < S - 1; s++) {
-    with_radix(ax.radix[s], [&](auto tag) {
-      constexpr int R = decltype(tag)::value;
-      if (s == 0) run_stage<R, false, false, W>(n, L, ax.tw, ldg, sst);
-      else run_stage<R, false, false, W>(n, L, ax.tw, sld, sst);
-    });
-    L /= ax.radix[s];
-    __syncthreads();
-  }
-  with_radix(ax.radix[S - 1], [&](auto tag) {
-    constexpr int R = decltype(tag)::value;
-    if (S == 1) fused_filter_stage<R, W, C>(n, ldg, stg, filt);
-    else fused_filter_stage<R, W, C>(n, sld, sst, filt);
-  });
-  __syncthreads();
-  if (S > 1) dit_stages<true, W>(ax, sm, S - 2, stg);
+// 1/x for x > 0 by two Newton-Raphson steps y <- y + y*(1 - x*y) from the
+// single-precision reciprocal (about 2^-23 -> 2^-46 -> full double).
+__device__ __forceinline__ double recip_pos(double x) {
+  double y = (double)__frcp_rn((float)x);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
 }
 
-// ------------------------------------------------------------------ pass 5
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_zinv(const typename Cplx<T>::type *__restrict__ spec, T *__restrict__ out,
-                                                   const PassArgs<T> a) {
+// One tile per block: TMA brings the tile into shared memory, the stages run,
+// the last stage stores straight to HBM.  Blocks are dispatched in tile order
+// (consecutive kh tiles of one plane share DRAM rows), and several blocks per
+// SM overlap one another's loads and butterflies.
+template <typename T, int W, bool XPASS, bool INV, int NT, int N>
+__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1)
+    k_strided(const __grid_constant__ CUtensorMap tmap, typename Cplx<T>::type *dst, const PassArgs<T> a,
+              int box_rows) {
   using C = typename Cplx<T>::type;
-  constexpr int W = TileW<T>::value;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  C *sm = reinterpret_cast<C *>(smraw);
-  const long nlines = (long)a.ni * a.nj;
-  const long line0 = (long)blockIdx.x * (2 * W);
-  const int nk = a.nk;
-  const int *ipos = a.ax[2].ipos;
-
-  // Z[k] = A[k] + i B[k] over the Hermitian extension; the imaginary parts of
-  // the zero and Nyquist terms are dropped, as a C2R transform does.
-  for (int it = threadIdx.x; it < W * a.nh; it += blockDim.x) {
-    const int c = it % W;
-    const int k = it / W;
-    const long la = line0 + 2 * c;
-    C A = mk((T)0, (T)0), B = mk((T)0, (T)0);
-    if (la < nlines) A = spec[la * a.nhp + k];
-    if (la + 1 < nlines) B = spec[(la + 1) * a.nhp + k];
-    if (k == 0 || 2 * k == nk) {
-      sm[__ldg(ipos + k) * W + c] = mk(A.x, B.x);
-    } else {
-      sm[__ldg(ipos + k) * W + c] = mk(A.x - B.y, A.y + B.x);
-      sm[__ldg(ipos + nk - k) * W + c] = mk(A.x + B.y, B.x - A.y);
+  extern __shared__ unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar;
+  const AxisDev<C> &ax = XPASS ? a.ax[0] : a.ax[1];
+  const int n = N > 0 ? N : ax.n;
+  C *buf = reinterpret_cast<C *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+  const int ktiles = (a.nh + W - 1) / W;
+  const int t = blockIdx.x;
+  const int o = t / ktiles, kt = t - o * ktiles;
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+    mbar_expect_tx(&mbar, (uint32_t)(n * W * sizeof(C)));
+    for (int q = 0; q < n / box_rows; q++) {
+      if (XPASS) tma_load_3d(buf + q * box_rows * W, &tmap, 2 * W * kt, o, q * box_rows, &mbar);
+      else tma_load_3d(buf + q * box_rows * W, &tmap, 2 * W * kt, q * box_rows, o, &mbar);
     }
   }
-  __syncthreads();
-  auto stg = [&](int pos, int c, C v) {
-    const long la = line0 + 2 * c;
-    if (la < nlines) out[la * nk + pos] = v.x;
-    if (la + 1 < nlines) out[(la + 1) * nk + pos] = v.y;
-  };
-  dit_stages<true, W>(a.ax[2], sm, a.ax[2].nstages - 1, stg);
+  __syncthreads();   // barrier initialised before anyone polls it
+  const bool ok = mbar_wait_bounded(&mbar, 0);
+  if (__syncthreads_or(!ok)) {
+    // the copy never completed: report and give it a bounded chance to land
+    // before the block's shared memory is released
+    if (threadIdx.x == 0) {
+      atomicExch(a.status, kDevTmaTimeout);
+      mbar_wait_bounded(&mbar, 0);
+    }
+    return;
+  }
+  const int kh0 = kt * W;
+  const int ncol = min(W, a.nh - kh0);
+  PointTile<W, C> tile{buf};
+  const auto rl = rev_last<N>(ax);
+  if (!XPASS) {
+    const long base = (long)o * a.nj * a.nhp + kh0;
+    const int pitch = a.nhp;
+    auto gst = [&](int pos, int c, C v) {
+      if (c < ncol) dst[base + (long)rl(pos) * pitch + c] = v;
+    };
+    dif_all<N, INV, Map::ColFast, W, NT, false, false>(ax, tile, tile, gst, W);
+  } else {
+    const int j = o;
+    const long base = (long)j * a.nhp + kh0;
+    const long pitch = (long)a.nj * a.nhp;
+    auto gst = [&](int pos, int c, C v) {
+      if (c < ncol) dst[base + pos * pitch + c] = v;
+    };
+    // d = -1/((i2 + j2) + k2) with i2 = (min(i, ni-i)*ddi)^2 etc., as
+    // ParisPencil.cpp:276-279 forms it, times 1/N
+    const int ni = a.ni;
+    const double jd = double(min(j, a.nj - j)) * a.dd[1];
+    const double j2 = jd * jd;
+    const double ddi = a.dd[0], ddk = a.dd[2];
+    const double minvN = -a.invN;
+    auto filt = [&](int pos, int c, C v) -> C {
+      const int kx = rl(pos);
+      const int kh = kh0 + c;
+      if (c >= ncol) return v;
+      if ((kx | j | kh) == 0) return mk((T)0, (T)0);
+      const double id = double(min(kx, ni - kx)) * ddi;
+      const double kd = double(kh) * ddk;
+      const double d = recip_pos((id * id + j2) + kd * kd) * minvN;
+      return cscale(v, (T)d);
+    };
+    if constexpr (N > 0) {
+      constexpr int S = plan_stages(N);
+      constexpr int RF = plan_radix(N, S - 1);
+      if constexpr (S > 1) {
+        dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, true>(ax, tile, tile, tile, W);
+        fused_filter_stage<RF, W, NT, N, C>(N, tile, tile, filt);
+        __syncthreads();
+        dit_ct<N, S - 2, true, Map::ColFast, W, NT, true>(ax, tile, gst, W);
+      } else {
+        fused_filter_stage<RF, W, NT, N, C>(N, tile, gst, filt);
+      }
+    } else {
+      const int S = ax.nstages;
+      if (S > 1) dif_rt<false, Map::ColFast, W, NT, false>(ax, S - 1, tile, tile, tile, W);
+      with_radix(ax.radix[S - 1], [&](auto tag) {
+        constexpr int R = decltype(tag)::value;
+        if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, tile, gst, filt);
+        else fused_filter_stage<R, W, NT, 0, C>(n, tile, tile, filt);
+      });
+      __syncthreads();
+      if (S > 1) dit_rt<true, Map::ColFast, W, NT>(ax, S - 2, tile, gst, W);
+    }
+  }
 }
 
 // ------------------------------------------------------------- plan tables
@@ -236,6 +312,20 @@ __global__ void k_wavenumbers(int n, int count, int folded, double dd, double *k
 // ====================================================================== plan
 using namespace ff;
 
+namespace ff {
+
+// Launch shape of a persistent strided pass.
+struct StridedCfg {
+  int N;          // specialised length of the kernel, 0 = runtime plan
+  int threads;    // block size
+  int W;          // columns per tile
+  int box_rows;   // rows per TMA box (a divisor of n, at most 256)
+  size_t smem;    // dynamic shared memory: one tile + alignment slack
+  int grid;       // one block per tile
+};
+
+}  // namespace ff
+
 struct ff_plan {
   int n[3];
   int precision;
@@ -243,10 +333,17 @@ struct ff_plan {
   double dd[3];
   size_t bytes;
   int device;
+  int num_sms;
   void *dmem;
   AxisDev<double2> axd[3];
   AxisDev<float2> axf[3];
   double *kk[3];
+  int *status;
+  int zN;              // z passes: specialised length, 0 = runtime plan
+  int zW, zP;          // z passes: line pairs per block, line pitch in complex values
+  size_t zsmem;
+  unsigned ztiles;
+  StridedCfg ycfg, xcfg;
   cudaEvent_t ev[FF_NUM_PHASES + 1];
 };
 
@@ -259,17 +356,10 @@ bool smooth235(int n) {
   return n == 1;
 }
 
-// DIF radix order: 8s first, then a 4 or a 2, then 5s and 3s.
+// DIF radix order of the device plan (plan_radix in ff_fft.cuh).
 static std::vector<int> factor_radices(int n) {
   std::vector<int> r;
-  int twos = 0;
-  while (n % 2 == 0) { n /= 2; twos++; }
-  while (twos >= 3) { r.push_back(8); twos -= 3; }
-  if (twos == 2) r.push_back(4);
-  if (twos == 1) r.push_back(2);
-  while (n % 5 == 0) { r.push_back(5); n /= 5; }
-  while (n % 3 == 0) { r.push_back(3); n /= 3; }
-  if (r.empty()) r.push_back(1);
+  for (int s = 0; s < plan_stages(n); s++) r.push_back(plan_radix(n, s));
   return r;
 }
 
@@ -300,13 +390,138 @@ int set_error(int status, const char *fmt, ...) {
   return status;
 }
 
-template <typename T> static int set_smem_limits() {
-  const int lim = 227 * 1024;
-  FF_CUDA(cudaFuncSetAttribute(k_zfwd<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  FF_CUDA(cudaFuncSetAttribute(k_ypass<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  FF_CUDA(cudaFuncSetAttribute(k_ypass<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  FF_CUDA(cudaFuncSetAttribute(k_xpass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
-  FF_CUDA(cudaFuncSetAttribute(k_zinv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim));
+constexpr size_t kMaxDynSmem = 227 * 1024;   // per-block opt-in shared memory of sm_100
+
+// Raises fn's dynamic shared-memory limit to what is left beside its static
+// shared memory; returns that limit in *avail.
+template <typename F> static int allow_dyn_smem(F fn, size_t *avail) {
+  cudaFuncAttributes fa;
+  FF_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const size_t lim = kMaxDynSmem - fa.sharedSizeBytes;
+  FF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim));
+  if (avail) *avail = lim;
+  return FF_OK;
+}
+
+template <typename T>
+using StridedKernel = void (*)(const CUtensorMap, typename Cplx<T>::type *, const PassArgs<T>, int);
+template <typename T> using ZFwdKernel = void (*)(const T *, typename Cplx<T>::type *, const PassArgs<T>, int, int);
+template <typename T>
+using ZInvKernel = void (*)(const typename Cplx<T>::type *, T *, const PassArgs<T>, int, int);
+
+// The specialised length for an axis of n points, or 0 (runtime plan).
+static int special_n(int n) {
+#define FF_CASE(NN) if (n == NN) return NN;
+  FF_FOR_EACH_SPECIAL_N(FF_CASE)
+#undef FF_CASE
+  return 0;
+}
+
+template <typename T> static ZFwdKernel<T> zfwd_kernel(int N) {
+#define FF_CASE(NN) if (N == NN) return k_zfwd<T, NN>;
+  FF_FOR_EACH_SPECIAL_N(FF_CASE)
+#undef FF_CASE
+  return k_zfwd<T, 0>;
+}
+template <typename T> static ZInvKernel<T> zinv_kernel(int N) {
+#define FF_CASE(NN) if (N == NN) return k_zinv<T, NN>;
+  FF_FOR_EACH_SPECIAL_N(FF_CASE)
+#undef FF_CASE
+  return k_zinv<T, 0>;
+}
+
+// kind: 0 = y forward, 1 = y inverse, 2 = x (forward, filter, inverse);
+// 128-byte rows (W = 8 FP64 / 16 FP32), 256 threads.
+template <typename T, int N> static StridedKernel<T> strided_n(int kind) {
+  constexpr int W = 128 / (2 * (int)sizeof(T));
+  return kind == 0 ? k_strided<T, W, false, false, 256, N>
+                   : kind == 1 ? k_strided<T, W, false, true, 256, N> : k_strided<T, W, true, false, 256, N>;
+}
+template <typename T> static StridedKernel<T> strided_kernel(int kind, int N) {
+#define FF_CASE(NN) if (N == NN) return strided_n<T, NN>(kind);
+  FF_FOR_EACH_SPECIAL_N(FF_CASE)
+#undef FF_CASE
+  return strided_n<T, 0>(kind);
+}
+
+// Largest divisor d of n with d <= cap and d % step == 0 (0 if none).
+static int largest_divisor_at_most(int n, int cap, int step) {
+  for (int d = std::min(n, cap); d >= 1; d--)
+    if (n % d == 0 && d % step == 0) return d;
+  return 0;
+}
+
+template <typename T> static int configure(ff_plan *p) {
+  using C = typename Cplx<T>::type;
+  const size_t csz = sizeof(C);
+  // z passes: W line pairs, two line-major buffers of pitch P, ~64 KB per block
+  const int align = csz == 16 ? 8 : 16;
+  p->zN = special_n(p->n[2]);
+  p->zP = (p->n[2] + align - 1) / align * align;
+  const size_t per_pair = 2 * (size_t)p->zP * csz;
+  p->zW = (int)std::max<size_t>(1, std::min<size_t>(8, (64 * 1024) / per_pair));
+  p->zsmem = p->zW * per_pair;
+  const long npairs = ((long)p->n[0] * p->n[1] + 1) / 2;
+  p->ztiles = (unsigned)((npairs + p->zW - 1) / p->zW);
+  int rc = allow_dyn_smem(zfwd_kernel<T>(p->zN), nullptr);
+  if (rc == FF_OK) rc = allow_dyn_smem(zinv_kernel<T>(p->zN), nullptr);
+  if (rc != FF_OK) return rc;
+  // strided passes: one tile of W 128-byte columns x n rows per block
+  const int W = 128 / (int)csz;
+  for (int kind = 0; kind < 3; kind++) {
+    StridedCfg &cfg = kind == 2 ? p->xcfg : p->ycfg;
+    const int n = kind == 2 ? p->n[0] : p->n[1];
+    cfg.N = special_n(n);
+    cfg.threads = 256;
+    cfg.W = W;
+    cfg.box_rows = largest_divisor_at_most(n, 256, 1);
+    cfg.smem = (size_t)n * W * csz + 128;
+    StridedKernel<T> fn = strided_kernel<T>(kind, cfg.N);
+    size_t avail = 0;
+    rc = allow_dyn_smem(fn, &avail);
+    if (rc != FF_OK) return rc;
+    if (cfg.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "no tile shape for an axis of %d points", n);
+    const long ktiles = (p->nh + W - 1) / W;
+    cfg.grid = (int)((kind == 2 ? p->n[1] : p->n[0]) * ktiles);
+  }
+  return FF_OK;
+}
+
+// cuTensorMapEncodeTiled, fetched from the driver through the runtime.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
+// Tensor map of a half spectrum at `base` viewed as (2*nh reals, nj, ni) with
+// row pitch nhp complex values; box = one tile chunk of the y or x pass.
+template <typename T> static int spectrum_map(const ff_plan *p, void *base, const StridedCfg &cfg, bool xpass,
+                                              CUtensorMap *map) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return set_error(FF_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint64_t csz = 2 * sizeof(T);
+  cuuint64_t dims[3] = {(cuuint64_t)2 * p->nh, (cuuint64_t)p->n[1], (cuuint64_t)p->n[0]};
+  cuuint64_t strides[2] = {(cuuint64_t)p->nhp * csz, (cuuint64_t)p->nhp * csz * p->n[1]};
+  cuuint32_t box[3] = {(cuuint32_t)(2 * cfg.W), xpass ? 1u : (cuuint32_t)cfg.box_rows,
+                       xpass ? (cuuint32_t)cfg.box_rows : 1u};
+  cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  CUresult r = enc(map, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(FF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return FF_OK;
 }
 
@@ -323,41 +538,56 @@ template <typename T> static PassArgs<T> pass_args(const ff_plan *p) {
     a.kk[d] = p->kk[d];
   }
   a.invN = 1.0 / (double(p->n[0]) * double(p->n[1]) * double(p->n[2]));
+  for (int d = 0; d < 3; d++) a.dd[d] = p->dd[d];
+  a.status = p->status;
   return a;
 }
 
 template <typename T>
 static int launch_solve(const ff_plan *p, void *density, void *potential, cudaStream_t st, bool timed) {
   using C = typename Cplx<T>::type;
-  constexpr int W = TileW<T>::value;
   const PassArgs<T> a = pass_args<T>(p);
-  const int ni = p->n[0], nj = p->n[1], nk = p->n[2];
-  const long npairs = ((long)ni * nj + 1) / 2;
-  const unsigned ztiles = (unsigned)((npairs + W - 1) / W);
-  const unsigned ktiles = (unsigned)((p->nh + W - 1) / W);
   T *D = static_cast<T *>(density);
   T *P = static_cast<T *>(potential);
   C *Ds = reinterpret_cast<C *>(density);
   C *Ps = reinterpret_cast<C *>(potential);
-  const size_t smz = (size_t)nk * W * sizeof(C);
-  const size_t smy = (size_t)nj * W * sizeof(C);
-  const size_t smx = (size_t)ni * W * sizeof(C);
+  CUtensorMap ymapP, xmapP;
+  int rc = spectrum_map<T>(p, potential, p->ycfg, false, &ymapP);
+  if (rc == FF_OK) rc = spectrum_map<T>(p, potential, p->xcfg, true, &xmapP);
+  if (rc != FF_OK) return rc;
   if (timed) FF_CUDA(cudaEventRecord(p->ev[0], st));
-  k_zfwd<T><<<ztiles, kThreads, smz, st>>>(D, Ps, a);
+  zfwd_kernel<T>(p->zN)<<<p->ztiles, kZThreads, p->zsmem, st>>>(D, Ps, a, p->zW, p->zP);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[1], st));
-  k_ypass<T, false><<<dim3(ktiles, ni), kThreads, smy, st>>>(Ps, Ps, a);
+  strided_kernel<T>(0, p->ycfg.N)<<<p->ycfg.grid, p->ycfg.threads, p->ycfg.smem, st>>>(ymapP, Ps, a,
+                                                                                       p->ycfg.box_rows);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[2], st));
-  k_xpass<T><<<dim3(ktiles, nj), kThreads, smx, st>>>(Ps, a);
+  strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, p->xcfg.threads, p->xcfg.smem, st>>>(xmapP, Ps, a,
+                                                                                       p->xcfg.box_rows);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[3], st));
-  k_ypass<T, true><<<dim3(ktiles, ni), kThreads, smy, st>>>(Ps, Ds, a);
+  strided_kernel<T>(1, p->ycfg.N)<<<p->ycfg.grid, p->ycfg.threads, p->ycfg.smem, st>>>(ymapP, Ds, a,
+                                                                                       p->ycfg.box_rows);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[4], st));
-  k_zinv<T><<<ztiles, kThreads, smz, st>>>(Ds, P, a);
+  zinv_kernel<T>(p->zN)<<<p->ztiles, kZThreads, p->zsmem, st>>>(Ds, P, a, p->zW, p->zP);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[5], st));
+  return FF_OK;
+}
+
+// Reads and clears the device status word; FF_ERR_TIMEOUT if a bounded wait
+// inside a kernel gave up.
+static int take_device_status(const ff_plan *p, cudaStream_t st) {
+  int h = 0;
+  FF_CUDA(cudaMemcpyAsync(&h, p->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FF_CUDA(cudaStreamSynchronize(st));
+  if (h != kDevOk) {
+    FF_CUDA(cudaMemsetAsync(p->status, 0, sizeof(int), st));
+    FF_CUDA(cudaStreamSynchronize(st));
+    return set_error(FF_ERR_TIMEOUT, "a TMA tile load did not complete within its wait limit (device status %d)", h);
+  }
   return FF_OK;
 }
 
@@ -365,7 +595,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
 
 extern "C" {
 
-const char *ff_version(void) { return "fishfry_b200 0.1 (sm_100a)"; }
+const char *ff_version(void) { return "fishfry_b200 0.2 (sm_100a)"; }
 
 const char *ff_last_error(void) { return g_err; }
 
@@ -408,7 +638,8 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
   std::memset(p, 0, sizeof(*p));
   for (int d = 0; d < 3; d++) {
     p->n[d] = n[d];
-    // ParisPencil.cpp:9-11
+    // ParisPencil.cpp:9-11; a one-point axis (hi == lo) has only wavenumber 0,
+    // where the reference's formula would give 0/0
     p->dd[d] = (n[d] > 1) ? 2.0 * M_PI * double(n[d] - 1) / (double(n[d]) * (hi[d] - lo[d])) : 0.0;
   }
   p->precision = precision;
@@ -419,12 +650,17 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
   const size_t spec = (size_t)n[0] * n[1] * p->nhp * csz;
   const size_t real = (size_t)n[0] * n[1] * n[2] * (csz / 2);
   p->bytes = std::max(spec, real);
-  cudaGetDevice(&p->device);
+  if (cudaGetDevice(&p->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess) {
+    delete p;
+    return set_error(FF_ERR_CUDA, "ff_plan_create: no current CUDA device");
+  }
 
-  // device tables: per axis tw (n complex), rev and ipos (n ints); kk per axis
+  // device tables: per axis tw (n complex), rev and ipos (n ints); kk per
+  // axis; one status word
   std::vector<int> radix[3], rev[3];
   size_t off = 0;
-  size_t o_tw[3], o_rev[3], o_ipos[3], o_kk[3];
+  size_t o_tw[3], o_tw64[3], o_rev[3], o_ipos[3], o_kk[3];
   auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~size_t(255); return o; };
   for (int d = 0; d < 3; d++) {
     radix[d] = factor_radices(n[d]);
@@ -434,10 +670,12 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
     }
     rev[d] = digit_reversal(n[d], radix[d]);
     o_tw[d] = take(n[d] * csz);
+    o_tw64[d] = precision == FF_FP64 ? o_tw[d] : take(n[d] * sizeof(double2));
     o_rev[d] = take(n[d] * sizeof(int));
     o_ipos[d] = take(n[d] * sizeof(int));
     o_kk[d] = take((d == 2 ? p->nh : n[d]) * sizeof(double));
   }
+  const size_t o_status = take(sizeof(int));
   for (int e = 0; e <= FF_NUM_PHASES; e++) {
     if (cudaEventCreate(&p->ev[e]) != cudaSuccess) {
       for (int q = 0; q < e; q++) cudaEventDestroy(p->ev[q]);
@@ -452,7 +690,9 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
     return set_error(FF_ERR_NOMEM, "ff_plan_create: cudaMalloc(%zu) for plan tables failed", off);
   }
   char *base = static_cast<char *>(p->dmem);
+  p->status = reinterpret_cast<int *>(base + o_status);
   int rc = FF_OK;
+  if (cudaMemset(p->status, 0, sizeof(int)) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_plan_create: memset");
   for (int d = 0; d < 3 && rc == FF_OK; d++) {
     std::vector<int> ipos(n[d]);
     for (int q = 0; q < n[d]; q++) ipos[rev[d][q]] = q;
@@ -460,8 +700,8 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
         cudaMemcpy(base + o_ipos[d], ipos.data(), n[d] * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
       rc = set_error(FF_ERR_CUDA, "ff_plan_create: table upload failed");
     const int blocks = std::min(1024, (n[d] + 255) / 256);
-    if (precision == FF_FP64) k_twiddles<<<blocks, 256>>>(n[d], reinterpret_cast<double2 *>(base + o_tw[d]));
-    else k_twiddles<<<blocks, 256>>>(n[d], reinterpret_cast<float2 *>(base + o_tw[d]));
+    k_twiddles<<<blocks, 256>>>(n[d], reinterpret_cast<double2 *>(base + o_tw64[d]));
+    if (precision == FF_FP32) k_twiddles<<<blocks, 256>>>(n[d], reinterpret_cast<float2 *>(base + o_tw[d]));
     const int cnt = d == 2 ? p->nh : n[d];
     k_wavenumbers<<<std::min(1024, (cnt + 255) / 256), 256>>>(n[d], cnt, d != 2, p->dd[d],
                                                               reinterpret_cast<double *>(base + o_kk[d]));
@@ -473,6 +713,7 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
     for (size_t s = 0; s < radix[d].size(); s++) ad.radix[s] = af.radix[s] = radix[d][s];
     ad.tw = reinterpret_cast<const double2 *>(base + o_tw[d]);
     af.tw = reinterpret_cast<const float2 *>(base + o_tw[d]);
+    ad.tw64 = af.tw64 = reinterpret_cast<const double2 *>(base + o_tw64[d]);
     ad.rev = af.rev = reinterpret_cast<const int *>(base + o_rev[d]);
     ad.ipos = af.ipos = reinterpret_cast<const int *>(base + o_ipos[d]);
     p->axd[d] = ad;
@@ -481,7 +722,7 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
   if (rc == FF_OK && cudaGetLastError() != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_plan_create: table kernels");
   if (rc == FF_OK && cudaDeviceSynchronize() != cudaSuccess)
     rc = set_error(FF_ERR_CUDA, "ff_plan_create: synchronize failed");
-  if (rc == FF_OK) rc = precision == FF_FP64 ? set_smem_limits<double>() : set_smem_limits<float>();
+  if (rc == FF_OK) rc = precision == FF_FP64 ? configure<double>(p) : configure<float>(p);
   if (rc != FF_OK) {
     ff_plan_destroy(p);
     return rc;
@@ -526,8 +767,14 @@ int ff_solve(const ff_plan *p, size_t bytes, void *density, void *potential, voi
     float tot = 0;
     FF_CUDA(cudaEventElapsedTime(&tot, p->ev[0], p->ev[FF_NUM_PHASES]));
     times->total_ms = tot;
+    return take_device_status(p, st);
   }
   return FF_OK;
+}
+
+int ff_plan_check(const ff_plan *p, void *stream) {
+  if (!p) return set_error(FF_ERR_INVALID, "ff_plan_check: null plan");
+  return take_device_status(p, static_cast<cudaStream_t>(stream));
 }
 
 int ff_plan_destroy(ff_plan *p) {

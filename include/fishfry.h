@@ -92,6 +92,12 @@ int ff_plan_info(const ff_plan *plan, int n[3], int *precision);
 int ff_solve(const ff_plan *plan, size_t bytes, void *density, void *potential, void *stream,
              ff_phase_times *times);
 
+/* Reads and clears the plan's device status word (waits for `stream`).
+ * Returns FF_ERR_TIMEOUT if a bounded wait inside a solve kernel gave up since
+ * the last check (a TMA tile copy that never completed); that solve's result
+ * is invalid.  ff_solve with `times` runs this check itself. */
+int ff_plan_check(const ff_plan *plan, void *stream);
+
 int ff_plan_destroy(ff_plan *plan);
 
 /* Harness: write f on the device at x = xlo + i*dx (FishFry.hpp:22-44),

@@ -135,8 +135,8 @@ def test_oracle_matches_reference_golden(oracle, path):
     norms = oracle.rel_norms(oracle.solve(f))
     ref_norms = g["rel_norms"]
     for a, b in zip(norms, ref_norms):
-        if b > 1e-10:        # truncation-dominated: must agree to many digits
-            assert abs(a - b) <= 1e-9 * b
+        if b > 1e-10:        # truncation-dominated: equal up to the round-off in d
+            assert abs(a - b) <= 1e-7 * b
         else:                # round-off level on both sides
             assert a < 1e-13 and b < 1e-13
 

@@ -45,7 +45,8 @@ def rel_l2(a, b):
 
 PARITY_SIZES = [(8, 8, 8), (16, 16, 16), (12, 10, 8), (5, 9, 6), (2, 3, 5), (1, 4, 6), (3, 1, 1), (1, 1, 2),
                 (30, 45, 50), (64, 48, 40), (64, 64, 64), (100, 36, 27), (96, 80, 75), (128, 128, 128),
-                (45, 81, 125), (256, 96, 72), (1800, 2, 4), (4, 1800, 6), (6, 5, 1800), (243, 16, 10)]
+                (45, 81, 125), (256, 96, 72), (1800, 2, 4), (4, 1800, 6), (6, 5, 1800), (243, 16, 10),
+                (1024, 8, 10), (6, 960, 9), (1215, 4, 6), (3, 1125, 4), (1125, 3, 1215)]
 
 
 @pytest.mark.parametrize("n", PARITY_SIZES)
