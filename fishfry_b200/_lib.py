@@ -26,7 +26,8 @@ FF_MAX_AXIS = 1800
 # Every symbol include/fishfry.h declares.
 EXPORTS = [
     "ff_phase_name", "ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
-    "ff_init_field", "ff_error_sums", "ff_modes_generate", "ff_status_string", "ff_last_error", "ff_version",
+    "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_status_string",
+    "ff_last_error", "ff_version",
 ]
 
 
@@ -64,13 +65,14 @@ def _declare(L):
     L.ff_plan_destroy.argtypes = [vp]
     L.ff_init_field.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, vp]
     L.ff_error_sums.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, d3, vp]
+    L.ff_error_sums_noalloc.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, d3, vp]
     L.ff_modes_generate.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, i3, ctypes.c_double, vp]
     L.ff_status_string.argtypes = [ctypes.c_int]
     L.ff_status_string.restype = ctypes.c_char_p
     L.ff_last_error.restype = ctypes.c_char_p
     L.ff_version.restype = ctypes.c_char_p
     for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
-                 "ff_init_field", "ff_error_sums", "ff_modes_generate"):
+                 "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate"):
         getattr(L, name).restype = ctypes.c_int
 
 

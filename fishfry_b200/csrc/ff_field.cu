@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "ff_status.hpp"
 
@@ -175,6 +176,87 @@ static unsigned grid_for(long N, int threads) {
   return (unsigned)(b < 148L * 32 ? (b < 1 ? 1 : b) : 148L * 32);
 }
 
+// ---------------------------------------------------------------------------
+// Error sums without any device allocation.
+//
+// Some callers cannot allocate device memory at the point where they want the
+// error norms: a host application whose own pool allocator has already
+// reserved the device memory, a time-critical loop where cudaMalloc's implicit
+// device synchronisation is not acceptable, or plug-in code that may not call
+// the CUDA allocator at all.  For them the partial sums live in a fixed
+// file-scope device array instead of a per-call buffer: every GPU that loads
+// this library holds it (about 384 KB) until the process exits.
+//
+// Each block reduces one contiguous chunk of kNoAllocChunk points in a fixed
+// order, so the number of partials, and the array's size, bound the grid:
+// at most kNoAllocMaxChunks * kNoAllocChunk = 2^30 points (1024^3).
+constexpr long kNoAllocChunk = 65536;
+constexpr int kNoAllocMaxChunks = 16384;
+static __device__ __align__(256) double g_noalloc_partials[3 * kNoAllocMaxChunks + 3];
+
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads) k_diff_chunks(const FieldArgs a, const T *__restrict__ phi,
+                                                             double *__restrict__ partial) {
+  __shared__ double s1[kSumThreads], s2[kSumThreads], sm[kSumThreads];
+  const long N = (long)a.ni * a.nj * a.nk;
+  const long q0 = (long)blockIdx.x * kNoAllocChunk;
+  const long q1 = q0 + kNoAllocChunk < N ? q0 + kNoAllocChunk : N;
+  double t1 = 0, t2 = 0, tm = 0;
+  for (long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+    const int k = (int)(q % a.nk);
+    const long ij = q / a.nk;
+    const int j = (int)(ij % a.nj);
+    const int i = (int)(ij / a.nj);
+    const PointFactors p = factors(a, i, j, k);
+    double ex = p.px * p.py * p.pz;
+    if (a.nmodes) ex += modes_sum(a, i, j, k, true);
+    const double d = fabs(ex - (phi ? (double)phi[q] : 0.0));
+    t1 += d;
+    t2 += d * d;
+    tm = (d > tm || d != d) ? d : tm;
+  }
+  s1[threadIdx.x] = t1;
+  s2[threadIdx.x] = t2;
+  sm[threadIdx.x] = tm;
+  __syncthreads();
+  for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+      const double o = sm[threadIdx.x + w];
+      if (o > sm[threadIdx.x] || o != o) sm[threadIdx.x] = o;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[3 * blockIdx.x + 0] = s1[0];
+    partial[3 * blockIdx.x + 1] = s2[0];
+    partial[3 * blockIdx.x + 2] = sm[0];
+  }
+}
+
+// Device address of g_noalloc_partials on the current device.  The name is a
+// host-side stand-in, not a device address, so it is looked up once per
+// device (with that device current) and remembered.
+static int noalloc_partials(double **out) {
+  static std::mutex mu;
+  static void *addr[256] = {};
+  int dev = 0;
+  FF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return set_error(FF_ERR_INVALID, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess)
+      return set_error(FF_ERR_CUDA, "cudaGetSymbolAddress of the static partial-sum array failed: %s",
+                       cudaGetErrorString(e));
+    addr[dev] = p;
+  }
+  *out = static_cast<double *>(addr[dev]);
+  return FF_OK;
+}
+
 }  // namespace ff
 
 using namespace ff;
@@ -221,6 +303,43 @@ int ff_error_sums(const int n[3], const double xlo[3], const double dx[3], int n
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess)
     return set_error(FF_ERR_CUDA, "ff_error_sums: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
+  sums[0] = host[0];
+  sums[1] = host[1];
+  sums[2] = host[2];
+  return FF_OK;
+}
+
+int ff_error_sums_noalloc(const int n[3], const double xlo[3], const double dx[3], int nmodes,
+                          const ff_mode *modes, int precision, const void *phi, double sums[3], void *stream) {
+  FieldArgs a;
+  int rc = field_args(n, xlo, dx, nmodes, modes, a);
+  if (rc != FF_OK) return rc;
+  if (!sums) return set_error(FF_ERR_INVALID, "ff_error_sums_noalloc: null sums");
+  if (precision != FF_FP64 && precision != FF_FP32)
+    return set_error(FF_ERR_INVALID, "ff_error_sums_noalloc: bad precision %d", precision);
+  const long N = (long)n[0] * n[1] * n[2];
+  const long chunks = (N + kNoAllocChunk - 1) / kNoAllocChunk;
+  if (chunks > kNoAllocMaxChunks)
+    return set_error(FF_ERR_UNSUPPORTED,
+                     "ff_error_sums_noalloc: %ld points exceed the fixed partial-sum array (at most %ld points)", N,
+                     (long)kNoAllocMaxChunks * kNoAllocChunk);
+  double *partial = nullptr;
+  rc = noalloc_partials(&partial);
+  if (rc != FF_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // every slot read below is written by this call first: nothing to clear
+  if (precision == FF_FP64)
+    k_diff_chunks<double><<<(unsigned)chunks, kSumThreads, 0, st>>>(a, static_cast<const double *>(phi), partial);
+  else
+    k_diff_chunks<float><<<(unsigned)chunks, kSumThreads, 0, st>>>(a, static_cast<const float *>(phi), partial);
+  double *total = partial + 3 * kNoAllocMaxChunks;
+  k_diff_final<<<1, kSumThreads, 0, st>>>(partial, (int)chunks, total);
+  cudaError_t e = cudaGetLastError();
+  double host[3] = {0, 0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, total, sizeof(host), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess)
+    return set_error(FF_ERR_CUDA, "ff_error_sums_noalloc: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
   sums[0] = host[0];
   sums[1] = host[1];
   sums[2] = host[2];

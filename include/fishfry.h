@@ -114,6 +114,23 @@ int ff_init_field(const int n[3], const double xlo[3], const double dx[3], int n
 int ff_error_sums(const int n[3], const double xlo[3], const double dx[3], int nmodes,
                   const ff_mode *modes, int precision, const void *phi, double sums[3], void *stream);
 
+/* ff_error_sums for callers that cannot allocate device memory (no counterpart
+ * in the reference).  Some callers may not allocate at the point where they
+ * want the norms: their host application's pool allocator already holds the
+ * device memory, cudaMalloc's implicit synchronisation is unacceptable in their
+ * loop, or they are plug-ins that may not call the CUDA allocator at all.
+ * This entry point calls no cudaMalloc/cudaFree: its partial sums live in a
+ * fixed device array inside the library (about 384 KB per GPU, held until the
+ * process exits), so grids are limited to 2^30 points (1024^3); larger ones
+ * return FF_ERR_UNSUPPORTED.  Same arguments and results as ff_error_sums,
+ * summed in a different fixed order (so sums agree to rounding, max exactly).
+ * The first call on each device looks up that array's device address; make it
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  sums is HOST memory; the call waits for stream. */
+int ff_error_sums_noalloc(const int n[3], const double xlo[3], const double dx[3], int nmodes,
+                          const ff_mode *modes, int precision, const void *phi, double sums[3], void *stream);
+
 /* Seeded random modes: `count` modes with integer k, 0 < |k| <= kmax and
  * |k_axis| <= kaxis[axis]; amplitude ~ N(0, sigma), phase ~ U[0, 2*pi)
  * (SplitMix64 counter stream + Box-Muller).  Host only. */
