@@ -20,12 +20,13 @@ FF_ERR_TASKS = 7
 
 FF_FP64 = 0
 FF_FP32 = 1
-FF_NUM_PHASES = 5
+FF_MAX_PHASES = 5
 FF_MAX_AXIS = 1800
 
 # Every symbol include/fishfry.h declares.
 EXPORTS = [
-    "ff_phase_name", "ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
+    "ff_phase_name", "ff_plan_phases", "ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check",
+    "ff_plan_destroy",
     "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_status_string",
     "ff_last_error", "ff_version",
 ]
@@ -45,7 +46,7 @@ class Mode(ctypes.Structure):
 
 
 class PhaseTimes(ctypes.Structure):
-    _fields_ = [("ms", ctypes.c_double * FF_NUM_PHASES), ("total_ms", ctypes.c_double)]
+    _fields_ = [("count", ctypes.c_int), ("ms", ctypes.c_double * FF_MAX_PHASES), ("total_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -55,8 +56,10 @@ def _declare(L):
     i3 = ctypes.POINTER(ctypes.c_int)
     d3 = ctypes.POINTER(ctypes.c_double)
     vp = ctypes.c_void_p
-    L.ff_phase_name.argtypes = [ctypes.c_int]
+    L.ff_phase_name.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.ff_phase_name.restype = ctypes.c_char_p
+    L.ff_plan_phases.argtypes = [ctypes.c_void_p]
+    L.ff_plan_phases.restype = ctypes.c_int
     L.ff_plan_create.argtypes = [i3, d3, d3, ctypes.c_int, ctypes.POINTER(vp)]
     L.ff_plan_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
     L.ff_plan_info.argtypes = [vp, i3, i3]

@@ -10,7 +10,7 @@ import math
 import time
 
 from . import _lib
-from ._lib import FF_FP32, FF_FP64, FF_NUM_PHASES, FFError, check, dbl3, int3, lib, modes_array
+from ._lib import FF_FP32, FF_FP64, FFError, check, dbl3, int3, lib, modes_array
 
 
 def _ptr(buf):
@@ -38,8 +38,10 @@ def reference_domain(n):
     return lo, hi, list(lo), dx
 
 
-def phase_names():
-    return [lib().ff_phase_name(p).decode() for p in range(FF_NUM_PHASES)]
+def phase_names(plan):
+    """Names of the plan's device launches (3 fused passes, or 5 passes)."""
+    h = plan.handle if isinstance(plan, Plan) else plan._plan.handle
+    return [lib().ff_phase_name(h, q).decode() for q in range(lib().ff_plan_phases(h))]
 
 
 class Plan:
@@ -72,8 +74,11 @@ class Plan:
         check(lib().ff_solve(self._h, nb, _ptr(density), _ptr(potential), _stream(stream),
                              ctypes.byref(times) if timed else None), "ff_solve")
         if timed:
-            return list(times.ms), times.total_ms
+            return list(times.ms)[:times.count], times.total_ms
         return None
+
+    def phases(self):
+        return lib().ff_plan_phases(self._h)
 
     def check(self, stream=None):
         """Raises FFError(FF_ERR_TIMEOUT) if a kernel's bounded wait gave up."""
@@ -113,7 +118,7 @@ class ParisPencil:
         stamps.append(("Total", t0))
         ms, _ = self._plan.solve(density, potential, nbytes=bytes, timed=True)
         t = t0
-        for name, dt in zip(phase_names(), ms):
+        for name, dt in zip(phase_names(self._plan), ms):
             t += 1e-3 * dt
             stamps.append((name, t))
 

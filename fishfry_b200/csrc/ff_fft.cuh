@@ -495,7 +495,31 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int x, 
       : "memory");
 }
 
+// 3-D tiled TMA store of one box from shared memory (bulk async-group).
+__device__ __forceinline__ void tma_store_3d(const void *tmap, int x, int y, int z, const void *src) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(tmap), "r"(x),
+               "r"(y), "r"(z), "r"(smem_u32(src))
+               : "memory");
+}
+
+// Contiguous bulk copies (addresses 16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *m) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(m))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until every committed bulk store of this thread has finished reading
+// shared memory (the buffer may then be reused or released).
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
 // Device-side status word values (plan status buffer).
-enum : int { kDevOk = 0, kDevTmaTimeout = 1 };
+enum : int { kDevOk = 0, kDevTmaTimeout = 1, kDevDepTimeout = 2 };
 
 }  // namespace ff

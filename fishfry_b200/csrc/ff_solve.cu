@@ -60,101 +60,223 @@ template <int N, typename C> __device__ __forceinline__ typename RevLastOf<N>::t
   }
 }
 
-// ------------------------------------------------------------------ pass 1
-// Tile: W line pairs (2W consecutive real lines), two line-major buffers A, B
-// of pitch P.  Line pair c is transformed as z = f[line a] + i f[line b].
-template <typename T, int N>
-__global__ void __launch_bounds__(kZThreads) k_zfwd(const T *__restrict__ f, typename Cplx<T>::type *__restrict__ spec,
-                                                    const PassArgs<T> a, int W, int P) {
-  using C = typename Cplx<T>::type;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  C *A = reinterpret_cast<C *>(smraw);
-  C *B = A + W * P;
-  const long nlines = (long)a.ni * a.nj;
-  const long line0 = (long)blockIdx.x * (2 * W);
-  const int nk = N > 0 ? N : a.nk;
-  const AxisDev<C> &ax = a.ax[2];
+// ------------------------------------------------------------------ z tiles
+// A z tile is W line pairs held in two line-major buffers A, B of pitch P.
+// Pair c is lines (line0 + 2c, line0 + 2c + 1), transformed as
+// z = f[a] + i f[b]; lines at or past `lend` are absent (zero in, no output).
+//
+// With TMAIO the tile's lines enter and leave by bulk copies between HBM and
+// shared memory (the copy engine moves them; the threads only touch shared
+// memory), using the buffers as staging: the real lines land in B, the stages
+// run in A, the last stage writes B, and the output is staged in A.  Without
+// TMAIO the first stage reads HBM and the output is written from registers.
+// A holds max(W*P, 2W*nhp) complex values, B holds W*P (+ 128 bytes slack).
+struct ZTileIO {
+  uint64_t *mbar;      // TMAIO: barrier of the inbound copy
+  uint32_t parity;     // TMAIO: its phase
+  int *status;         // TMAIO: timeout report
+};
 
-  // stage 0 reads the two real lines straight from HBM, consecutive threads on
-  // consecutive points of one line
-  auto ldg = [&](int pos, int c) -> C {
-    const long la = line0 + 2 * c;
-    T x = 0, y = 0;
-    if (la < nlines) x = f[la * nk + pos];
-    if (la + 1 < nlines) y = f[(la + 1) * nk + pos];
-    return mk(x, y);
-  };
-  LineTile<C> tA{A, P}, tB{B, P};
-  LineTileRev<C, typename RevLastOf<N>::type> tBrev{tB, rev_last<N>(ax)};
-  dif_all<N, false, Map::PosFast, 1, kZThreads, true, false>(ax, ldg, tA, tBrev, W);   // B: Z in natural order
+// Inbound bulk copy of `bytes` (rounded up to 16) from src into dst, waited
+// for on every thread with an iteration limit.
+__device__ __forceinline__ bool bulk_in(void *dst, const void *src, size_t bytes, const ZTileIO &io) {
+  if (threadIdx.x == 0) {
+    const uint32_t b = (uint32_t)((bytes + 15) & ~size_t(15));
+    mbar_expect_tx(io.mbar, b);
+    bulk_load(dst, src, b, io.mbar);
+  }
+  const bool ok = mbar_wait_bounded(io.mbar, io.parity);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(io.status, kDevTmaTimeout);
+      mbar_wait_bounded(io.mbar, io.parity);
+    }
+    return false;
+  }
+  return true;
+}
 
-  // split: A[k] = (Z[k] + conj Z[n-k]) / 2,  B[k] = (Z[k] - conj Z[n-k]) / (2i)
-  const T h = (T)0.5;
-  const int nh = a.nh;
-  for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-    const int k = it % nh;
-    const int c = it / nh;
-    const long la = line0 + 2 * c;
-    if (la >= nlines) continue;
-    const C z = tB(k, c);
-    const C w = tB(k == 0 ? 0 : nk - k, c);
-    spec[la * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
-    if (la + 1 < nlines) spec[(la + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+// Outbound bulk copy of the staged bytes; a tail that is not a multiple of 16
+// bytes is stored by thread 0 itself.  Waits until the copy has read shared
+// memory.  The caller has fenced its shared-memory writes and barriered.
+template <typename E>
+__device__ __forceinline__ void bulk_out(E *dst, const E *src, size_t count) {
+  if (threadIdx.x == 0) {
+    const size_t bytes = count * sizeof(E);
+    const size_t body = bytes & ~size_t(15);
+    if (body) {
+      bulk_store(dst, src, (uint32_t)body);
+      bulk_commit();
+    }
+    for (size_t q = body / sizeof(E); q < count; q++) dst[q] = src[q];
+    if (body) bulk_wait_read();
   }
 }
 
-// ------------------------------------------------------------------ pass 5
-template <typename T, int N>
-__global__ void __launch_bounds__(kZThreads) k_zinv(const typename Cplx<T>::type *__restrict__ spec, T *__restrict__ out,
-                                                    const PassArgs<T> a, int W, int P) {
+// R2C along z (ParisPencil.cpp:152-165): the last stage writes Z in natural
+// order into B; the split A[k] = (Z[k] + conj Z[n-k]) / 2,
+// B[k] = (Z[k] - conj Z[n-k]) / (2i) goes out with consecutive threads on
+// consecutive k.
+template <typename T, int N, bool TMAIO>
+__device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cplx<T>::type *spec, const PassArgs<T> &a,
+                                           int W, int P, long line0, long lend, typename Cplx<T>::type *sm,
+                                           const ZTileIO &io) {
   using C = typename Cplx<T>::type;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  C *A = reinterpret_cast<C *>(smraw);
-  C *B = A + W * P;
-  const long nlines = (long)a.ni * a.nj;
-  const long line0 = (long)blockIdx.x * (2 * W);
   const int nk = N > 0 ? N : a.nk;
   const int nh = a.nh;
+  const int Asz = max(W * P, 2 * W * a.nhp);
+  C *A = sm;
+  C *B = A + ((Asz * (int)sizeof(C) + 127) & ~127) / (int)sizeof(C);
+  const int nl = (int)min((long)(2 * W), lend - line0);
   const AxisDev<C> &ax = a.ax[2];
   LineTile<C> tA{A, P}, tB{B, P};
   LineTileRev<C, typename RevLastOf<N>::type> tBrev{tB, rev_last<N>(ax)};
+  if constexpr (TMAIO) {
+    T *raw = reinterpret_cast<T *>(B);
+    if (!bulk_in(raw, f + line0 * nk, (size_t)nl * nk * sizeof(T), io)) return false;
+    auto ld0 = [&](int pos, int c) -> C {
+      const int la = 2 * c;
+      return mk(la < nl ? raw[la * nk + pos] : (T)0, la + 1 < nl ? raw[(la + 1) * nk + pos] : (T)0);
+    };
+    dif_all<N, false, Map::PosFast, 1, kZThreads, true, false>(ax, ld0, tA, tBrev, W);
+    // split into the staging rows [line][kh] (pitch nhp) in A, then one copy out
+    const T h = (T)0.5;
+    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+      const int k = it % nh;
+      const int c = it / nh;
+      const C z = tB(k, c);
+      const C w = tB(k == 0 ? 0 : nk - k, c);
+      A[(2 * c) * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
+      A[(2 * c + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    bulk_out(spec + line0 * a.nhp, A, (size_t)nl * a.nhp);
+    return true;
+  } else {
+    auto ldg = [&](int pos, int c) -> C {
+      const long la = line0 + 2 * c;
+      T x = 0, y = 0;
+      if (la < lend) x = f[la * nk + pos];
+      if (la + 1 < lend) y = f[(la + 1) * nk + pos];
+      return mk(x, y);
+    };
+    dif_all<N, false, Map::PosFast, 1, kZThreads, true, false>(ax, ldg, tA, tBrev, W);
+    const T h = (T)0.5;
+    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+      const int k = it % nh;
+      const int c = it / nh;
+      const long la = line0 + 2 * c;
+      if (la >= lend) continue;
+      const C z = tB(k, c);
+      const C w = tB(k == 0 ? 0 : nk - k, c);
+      spec[la * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
+      if (la + 1 < lend) spec[(la + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+    }
+    return true;
+  }
+}
 
-  // Z[k] = A[k] + i B[k] over the Hermitian extension, natural order in B; the
-  // imaginary parts of the zero and Nyquist terms are dropped, as a C2R
-  // transform does.
-  for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-    const int k = it % nh;
-    const int c = it / nh;
-    const long la = line0 + 2 * c;
-    C sa = mk((T)0, (T)0), sb = mk((T)0, (T)0);
-    if (la < nlines) sa = spec[la * a.nhp + k];
-    if (la + 1 < nlines) sb = spec[(la + 1) * a.nhp + k];
+// C2R along z (ParisPencil.cpp:368-380): Z[k] = A[k] + i B[k] over the
+// Hermitian extension in natural order in B (the imaginary parts of the zero
+// and Nyquist terms are dropped, as a C2R transform does), inverse DIF into
+// natural order in B, real and imaginary parts out to the two lines.
+template <typename T, int N, bool TMAIO>
+__device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T *__restrict__ out,
+                                           const PassArgs<T> &a, int W, int P, long line0, long lend,
+                                           typename Cplx<T>::type *sm, const ZTileIO &io) {
+  using C = typename Cplx<T>::type;
+  const int nk = N > 0 ? N : a.nk;
+  const int nh = a.nh;
+  const int Asz = max(W * P, 2 * W * a.nhp);
+  C *A = sm;
+  C *B = A + ((Asz * (int)sizeof(C) + 127) & ~127) / (int)sizeof(C);
+  const int nl = (int)min((long)(2 * W), lend - line0);
+  const AxisDev<C> &ax = a.ax[2];
+  LineTile<C> tA{A, P}, tB{B, P};
+  LineTileRev<C, typename RevLastOf<N>::type> tBrev{tB, rev_last<N>(ax)};
+  auto hermitian = [&](int k, int c, C sa, C sb) {
     if (k == 0 || 2 * k == nk) {
       tB(k, c, mk(sa.x, sb.x));
     } else {
       tB(k, c, mk(sa.x - sb.y, sa.y + sb.x));
       tB(nk - k, c, mk(sa.x + sb.y, sb.x - sa.y));
     }
-  }
-  __syncthreads();
-  dif_all<N, true, Map::PosFast, 1, kZThreads, true, false>(ax, tB, tA, tBrev, W);   // B: z in natural order
-
-  for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
-    const int t = it % nk;
-    const int c = it / nk;
-    const long la = line0 + 2 * c;
-    const C v = tB(t, c);
-    if (la < nlines) out[la * nk + t] = v.x;
-    if (la + 1 < nlines) out[(la + 1) * nk + t] = v.y;
+  };
+  if constexpr (TMAIO) {
+    if (!bulk_in(A, spec + line0 * a.nhp, (size_t)nl * a.nhp * sizeof(C), io)) return false;
+    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+      const int k = it % nh;
+      const int c = it / nh;
+      const int la = 2 * c;
+      const C sa = la < nl ? A[la * a.nhp + k] : mk((T)0, (T)0);
+      const C sb = la + 1 < nl ? A[(la + 1) * a.nhp + k] : mk((T)0, (T)0);
+      hermitian(k, c, sa, sb);
+    }
+    __syncthreads();
+    dif_all<N, true, Map::PosFast, 1, kZThreads, true, false>(ax, tB, tA, tBrev, W);
+    // real lines staged in A, then one copy out
+    T *raw = reinterpret_cast<T *>(A);
+    for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
+      const int t = it % nk;
+      const int c = it / nk;
+      const C v = tB(t, c);
+      raw[(2 * c) * nk + t] = v.x;
+      raw[(2 * c + 1) * nk + t] = v.y;
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    bulk_out(out + line0 * nk, raw, (size_t)nl * nk);
+    return true;
+  } else {
+    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+      const int k = it % nh;
+      const int c = it / nh;
+      const long la = line0 + 2 * c;
+      C sa = mk((T)0, (T)0), sb = mk((T)0, (T)0);
+      if (la < lend) sa = __ldcg(spec + la * a.nhp + k);
+      if (la + 1 < lend) sb = __ldcg(spec + (la + 1) * a.nhp + k);
+      hermitian(k, c, sa, sb);
+    }
+    __syncthreads();
+    dif_all<N, true, Map::PosFast, 1, kZThreads, true, false>(ax, tB, tA, tBrev, W);
+    for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
+      const int t = it % nk;
+      const int c = it / nk;
+      const long la = line0 + 2 * c;
+      const C v = tB(t, c);
+      if (la < lend) out[la * nk + t] = v.x;
+      if (la + 1 < lend) out[(la + 1) * nk + t] = v.y;
+    }
+    return true;
   }
 }
 
-// ------------------------------------------------------------- passes 2-4
-// Persistent strided pass.  A tile is W consecutive kh columns of all n rows
-// of one plane (y pass: fixed i, rows j; x pass: fixed j, rows i), held
-// point-major and brought in by TMA; results leave from registers straight
-// to HBM in the last stage.
-//
+// --------------------------------------------------------- strided tiles
+// A strided tile is W consecutive kh columns (128-byte rows) of all n rows of
+// one plane, held point-major: y tiles are (plane i, rows j), x tiles are
+// (plane j, rows i).
+
+// y transform of one tile; stage 0 reads through ld0 (the TMA-filled tile or
+// HBM/L2 directly), the last stage stores from registers straight to HBM at
+// the digit-reversed rows.
+template <typename T, int W, bool INV, int N, typename LD0>
+__device__ __forceinline__ void y_tile(LD0 &ld0, typename Cplx<T>::type *dst, const PassArgs<T> &a, int o, int kt,
+                                       typename Cplx<T>::type *sm) {
+  using C = typename Cplx<T>::type;
+  const AxisDev<C> &ax = a.ax[1];
+  const int kh0 = kt * W;
+  const int ncol = min(W, a.nh - kh0);
+  const long base = (long)o * a.nj * a.nhp + kh0;
+  const int pitch = a.nhp;
+  const auto rl = rev_last<N>(ax);
+  PointTile<W, C> tile{sm};
+  auto gst = [&](int pos, int c, C v) {
+    if (c < ncol) dst[base + (long)rl(pos) * pitch + c] = v;
+  };
+  dif_all<N, INV, Map::ColFast, W, kZThreads, false, false>(ax, ld0, tile, gst, W);
+}
+
 // The last DIF stage of the x forward transform, the filter and the first
 // DIT stage of the inverse act on the same register group.
 template <int R, int W, int NT, int NC, typename C, typename LD, typename ST, typename FL>
@@ -192,101 +314,329 @@ __device__ __forceinline__ double recip_pos(double x) {
   return fma(y, e, y);
 }
 
-// One tile per block: TMA brings the tile into shared memory, the stages run,
-// the last stage stores straight to HBM.  Blocks are dispatched in tile order
-// (consecutive kh tiles of one plane share DRAM rows), and several blocks per
-// SM overlap one another's loads and butterflies.
-template <typename T, int W, bool XPASS, bool INV, int NT, int N>
-__global__ void __launch_bounds__(NT, NT == 256 ? 3 : 1)
+// x transform of one TMA-filled tile: forward, filter, inverse.  The inverse
+// ends in natural order in place, so the finished tile leaves by TMA stores
+// of the same boxes it came in with (columns past nh are clipped).
+template <typename T, int W, int N>
+__device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T> &a, int j, int kt, int box_rows,
+                                       typename Cplx<T>::type *sm) {
+  using C = typename Cplx<T>::type;
+  constexpr int NT = kZThreads;
+  const AxisDev<C> &ax = a.ax[0];
+  const int n = N > 0 ? N : ax.n;
+  const int kh0 = kt * W;
+  const int ncol = min(W, a.nh - kh0);
+  const auto rl = rev_last<N>(ax);
+  PointTile<W, C> tile{sm};
+  PointTile<W, C> &gst = tile;
+  // d = -1/((i2 + j2) + k2) with i2 = (min(i, ni-i)*ddi)^2 etc., as
+  // ParisPencil.cpp:276-279 forms it, times 1/N
+  const int ni = a.ni;
+  const double jd = double(min(j, a.nj - j)) * a.dd[1];
+  const double j2 = jd * jd;
+  const double ddi = a.dd[0], ddk = a.dd[2];
+  const double minvN = -a.invN;
+  auto filt = [&](int pos, int c, C v) -> C {
+    const int kx = rl(pos);
+    const int kh = kh0 + c;
+    if (c >= ncol) return v;
+    if ((kx | j | kh) == 0) return mk((T)0, (T)0);
+    const double id = double(min(kx, ni - kx)) * ddi;
+    const double kd = double(kh) * ddk;
+    const double d = recip_pos((id * id + j2) + kd * kd) * minvN;
+    return cscale(v, (T)d);
+  };
+  if constexpr (N > 0) {
+    constexpr int S = plan_stages(N);
+    constexpr int RF = plan_radix(N, S - 1);
+    if constexpr (S > 1) {
+      dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, true>(ax, tile, tile, tile, W);
+      fused_filter_stage<RF, W, NT, N, C>(N, tile, tile, filt);
+      __syncthreads();
+      dit_ct<N, S - 2, true, Map::ColFast, W, NT, true>(ax, tile, gst, W);
+    } else {
+      fused_filter_stage<RF, W, NT, N, C>(N, tile, gst, filt);
+    }
+  } else {
+    const int S = ax.nstages;
+    if (S > 1) dif_rt<false, Map::ColFast, W, NT, false>(ax, S - 1, tile, tile, tile, W);
+    with_radix(ax.radix[S - 1], [&](auto tag) {
+      constexpr int R = decltype(tag)::value;
+      if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, tile, gst, filt);
+      else fused_filter_stage<R, W, NT, 0, C>(n, tile, tile, filt);
+    });
+    __syncthreads();
+    if (S > 1) dit_rt<true, Map::ColFast, W, NT>(ax, S - 2, tile, gst, W);
+  }
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < n / box_rows; q++) tma_store_3d(tmap, 2 * W * kt, j, q * box_rows, sm + q * box_rows * W);
+    bulk_commit();
+    bulk_wait_read();
+  }
+}
+
+// Loads one strided tile with TMA into sm (boxes of box_rows rows) and waits
+// on mb for phase `parity` with an iteration limit.  Returns false on every
+// thread if the copy did not complete (the plan status word is set).  The
+// caller's earlier shared-memory accesses of sm must be fenced
+// (fence_proxy_async_smem) and barriered before the call.
+template <typename C, int W, bool XPASS>
+__device__ __forceinline__ bool tma_tile(const CUtensorMap *tmap, C *sm, uint64_t *mb, uint32_t parity, int n,
+                                         int box_rows, int o, int kt, int *status) {
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(mb, (uint32_t)(n * W * sizeof(C)));
+    for (int q = 0; q < n / box_rows; q++) {
+      if (XPASS) tma_load_3d(sm + q * box_rows * W, tmap, 2 * W * kt, o, q * box_rows, mb);
+      else tma_load_3d(sm + q * box_rows * W, tmap, 2 * W * kt, q * box_rows, o, mb);
+    }
+  }
+  const bool ok = mbar_wait_bounded(mb, parity);
+  if (__syncthreads_or(!ok)) {
+    // report, and give the copy in flight a bounded chance to land before the
+    // block's shared memory is released
+    if (threadIdx.x == 0) {
+      atomicExch(status, kDevTmaTimeout);
+      mbar_wait_bounded(mb, parity);
+    }
+    return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ unsigned char *align128(unsigned char *p) {
+  return reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+}
+
+// ------------------------------------------------- unfused pass kernels
+// (one launch per pass; used when the fused passes are switched off)
+// Specialised lengths move their z tiles with bulk copies (their line blocks
+// are always 16-byte aligned and have at least two stages); other lengths
+// read and write HBM from the threads.
+template <typename T, int N>
+__global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, typename Cplx<T>::type *spec,
+                                                       const PassArgs<T> a, int W, int P) {
+  extern __shared__ unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar;
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const long nlines = (long)a.ni * a.nj;
+  const ZTileIO io{&mbar, 0, a.status};
+  z_fwd_tile<T, N, (N > 0)>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+                            reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(kZThreads, 3) k_zinv(const typename Cplx<T>::type *spec, T *__restrict__ out,
+                                                       const PassArgs<T> a, int W, int P) {
+  extern __shared__ unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar;
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  const long nlines = (long)a.ni * a.nj;
+  const ZTileIO io{&mbar, 0, a.status};
+  z_inv_tile<T, N, (N > 0)>(spec, out, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+                            reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
+}
+
+// One TMA-loaded strided tile per block (y forward / inverse or x).  Blocks
+// are dispatched in tile order, so the kh tiles of one plane row, which share
+// DRAM rows, are fetched together.
+template <typename T, int W, bool XPASS, bool INV, int N>
+__global__ void __launch_bounds__(kZThreads, 3)
     k_strided(const __grid_constant__ CUtensorMap tmap, typename Cplx<T>::type *dst, const PassArgs<T> a,
               int box_rows) {
   using C = typename Cplx<T>::type;
   extern __shared__ unsigned char smraw[];
   __shared__ __align__(8) uint64_t mbar;
-  const AxisDev<C> &ax = XPASS ? a.ax[0] : a.ax[1];
-  const int n = N > 0 ? N : ax.n;
-  C *buf = reinterpret_cast<C *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+  C *sm = reinterpret_cast<C *>(align128(smraw));
+  const int n = N > 0 ? N : (XPASS ? a.ax[0].n : a.ax[1].n);
   const int ktiles = (a.nh + W - 1) / W;
-  const int t = blockIdx.x;
-  const int o = t / ktiles, kt = t - o * ktiles;
+  const int o = blockIdx.x / ktiles, kt = blockIdx.x - o * ktiles;
   if (threadIdx.x == 0) {
     mbar_init(&mbar, 1);
     mbar_init_fence();
-    mbar_expect_tx(&mbar, (uint32_t)(n * W * sizeof(C)));
-    for (int q = 0; q < n / box_rows; q++) {
-      if (XPASS) tma_load_3d(buf + q * box_rows * W, &tmap, 2 * W * kt, o, q * box_rows, &mbar);
-      else tma_load_3d(buf + q * box_rows * W, &tmap, 2 * W * kt, q * box_rows, o, &mbar);
-    }
   }
-  __syncthreads();   // barrier initialised before anyone polls it
-  const bool ok = mbar_wait_bounded(&mbar, 0);
-  if (__syncthreads_or(!ok)) {
-    // the copy never completed: report and give it a bounded chance to land
-    // before the block's shared memory is released
-    if (threadIdx.x == 0) {
-      atomicExch(a.status, kDevTmaTimeout);
-      mbar_wait_bounded(&mbar, 0);
-    }
+  __syncthreads();
+  if (!tma_tile<C, W, XPASS>(&tmap, sm, &mbar, 0, n, box_rows, o, kt, a.status)) return;
+  if (XPASS) {
+    x_tile<T, W, N>(&tmap, a, o, kt, box_rows, sm);
+  } else {
+    PointTile<W, C> tile{sm};
+    y_tile<T, W, INV, N>(tile, dst, a, o, kt, sm);
+  }
+}
+
+// ---------------------------------------------------------- fused passes
+// z forward + y forward (and y inverse + z inverse) in one persistent launch.
+// Blocks take tiles from an in-order work queue: the producer tiles of plane
+// i (z forward / y inverse) come `lag` planes ahead of its consumer tiles
+// (y forward / z inverse), and a consumer tile waits, with an iteration
+// limit, until the plane's producer count is complete.  The plane's
+// intermediate spectrum is therefore written and read back while it is still
+// in L2, and HBM sees the real field once and the spectrum once per
+// direction.  Every consumer waits only on tiles handed out before it, so the
+// queue cannot deadlock.
+struct FuseArgs {
+  int *ticket;     // work counter (zeroed before the launch)
+  int *done;       // per-plane producer counts (zeroed before the launch)
+  int planes;      // ni
+  int prod_pp;     // producer tiles per plane
+  int cons_pp;     // consumer tiles per plane
+  int lag;         // planes between a producer tile and its plane's consumers (<= planes)
+  int zW, zP;      // z tile shape
+  int box_rows;    // TMA box rows of y tiles
+};
+
+__device__ __forceinline__ void fuse_decode(const FuseArgs &f, int t, bool &cons, int &plane, int &tile) {
+  const int A = f.prod_pp, B = f.cons_pp, L = f.lag;
+  const int head = L * A;
+  if (t < head) {
+    cons = false;
+    plane = t / A;
+    tile = t - plane * A;
     return;
   }
-  const int kh0 = kt * W;
-  const int ncol = min(W, a.nh - kh0);
-  PointTile<W, C> tile{buf};
-  const auto rl = rev_last<N>(ax);
-  if (!XPASS) {
-    const long base = (long)o * a.nj * a.nhp + kh0;
-    const int pitch = a.nhp;
-    auto gst = [&](int pos, int c, C v) {
-      if (c < ncol) dst[base + (long)rl(pos) * pitch + c] = v;
-    };
-    dif_all<N, INV, Map::ColFast, W, NT, false, false>(ax, tile, tile, gst, W);
-  } else {
-    const int j = o;
-    const long base = (long)j * a.nhp + kh0;
-    const long pitch = (long)a.nj * a.nhp;
-    auto gst = [&](int pos, int c, C v) {
-      if (c < ncol) dst[base + pos * pitch + c] = v;
-    };
-    // d = -1/((i2 + j2) + k2) with i2 = (min(i, ni-i)*ddi)^2 etc., as
-    // ParisPencil.cpp:276-279 forms it, times 1/N
-    const int ni = a.ni;
-    const double jd = double(min(j, a.nj - j)) * a.dd[1];
-    const double j2 = jd * jd;
-    const double ddi = a.dd[0], ddk = a.dd[2];
-    const double minvN = -a.invN;
-    auto filt = [&](int pos, int c, C v) -> C {
-      const int kx = rl(pos);
-      const int kh = kh0 + c;
-      if (c >= ncol) return v;
-      if ((kx | j | kh) == 0) return mk((T)0, (T)0);
-      const double id = double(min(kx, ni - kx)) * ddi;
-      const double kd = double(kh) * ddk;
-      const double d = recip_pos((id * id + j2) + kd * kd) * minvN;
-      return cscale(v, (T)d);
-    };
-    if constexpr (N > 0) {
-      constexpr int S = plan_stages(N);
-      constexpr int RF = plan_radix(N, S - 1);
-      if constexpr (S > 1) {
-        dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, true>(ax, tile, tile, tile, W);
-        fused_filter_stage<RF, W, NT, N, C>(N, tile, tile, filt);
-        __syncthreads();
-        dit_ct<N, S - 2, true, Map::ColFast, W, NT, true>(ax, tile, gst, W);
-      } else {
-        fused_filter_stage<RF, W, NT, N, C>(N, tile, gst, filt);
-      }
+  t -= head;
+  const int mid = (f.planes - L) * (A + B);
+  if (t < mid) {
+    const int s = t / (A + B), q = t - s * (A + B);
+    cons = q >= A;
+    plane = cons ? s : L + s;
+    tile = cons ? q - A : q;
+    return;
+  }
+  t -= mid;
+  cons = true;
+  plane = (f.planes - L) + t / B;
+  tile = t - (t / B) * B;
+}
+
+// Bounded wait for *p >= target (acquire at GPU scope).
+__device__ __forceinline__ bool wait_count(const int *p, int target) {
+  for (int i = 0; i < (1 << 22); i++) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    if (v >= target) return true;
+    __nanosleep(128);
+  }
+  return false;
+}
+
+// Publishes this block's finished producer tile of `plane`.
+__device__ __forceinline__ void publish(int *done, int plane) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd(done + plane, 1);
+}
+
+// Waits for all producer tiles of `plane`; false on every thread on timeout.
+__device__ __forceinline__ bool await_plane(const FuseArgs &fa, int plane, int *status) {
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    ok = wait_count(fa.done + plane, fa.prod_pp);
+    if (!ok) atomicExch(status, kDevDepTimeout);
+  }
+  return !__syncthreads_or(!ok);
+}
+
+__device__ __forceinline__ int next_ticket(int *ticket, int *s_ticket) {
+  __syncthreads();   // the previous tile's shared-memory use is over
+  if (threadIdx.x == 0) *s_ticket = atomicAdd(ticket, 1);
+  __syncthreads();
+  return *s_ticket;
+}
+
+template <typename T, int NZ, int NY>
+__global__ void __launch_bounds__(kZThreads, 3)
+    k_zy_fwd(const T *__restrict__ f, typename Cplx<T>::type *spec, const PassArgs<T> a, const FuseArgs fa) {
+  using C = typename Cplx<T>::type;
+  constexpr int W = 128 / sizeof(C);
+  extern __shared__ unsigned char smraw[];
+  __shared__ int s_ticket;
+  C *sm = reinterpret_cast<C *>(align128(smraw));
+  const int total = fa.planes * (fa.prod_pp + fa.cons_pp);
+  for (;;) {
+    const int t = next_ticket(fa.ticket, &s_ticket);
+    if (t >= total) break;
+    bool cons;
+    int plane, tile;
+    fuse_decode(fa, t, cons, plane, tile);
+    if (!cons) {
+      const long first = (long)plane * a.nj;
+      z_fwd_tile<T, NZ, false>(f, spec, a, fa.zW, fa.zP, first + (long)tile * 2 * fa.zW, first + a.nj, sm,
+                               ZTileIO{nullptr, 0, a.status});
+      publish(fa.done, plane);
     } else {
-      const int S = ax.nstages;
-      if (S > 1) dif_rt<false, Map::ColFast, W, NT, false>(ax, S - 1, tile, tile, tile, W);
-      with_radix(ax.radix[S - 1], [&](auto tag) {
-        constexpr int R = decltype(tag)::value;
-        if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, tile, gst, filt);
-        else fused_filter_stage<R, W, NT, 0, C>(n, tile, tile, filt);
-      });
-      __syncthreads();
-      if (S > 1) dit_rt<true, Map::ColFast, W, NT>(ax, S - 2, tile, gst, W);
+      if (!await_plane(fa, plane, a.status)) break;
+      // the plane was written by other blocks moments ago: read it through L2
+      const int kh0 = tile * W;
+      const int ncol = min(W, a.nh - kh0);
+      const long base = (long)plane * a.nj * a.nhp + kh0;
+      const int pitch = a.nhp;
+      auto ldg = [&](int pos, int c) -> C {
+        return c < ncol ? __ldcg(spec + base + (long)pos * pitch + c) : mk((T)0, (T)0);
+      };
+      y_tile<T, W, false, NY>(ldg, spec, a, plane, tile, sm);
     }
   }
+}
+
+template <typename T, int NZ, int NY>
+__global__ void __launch_bounds__(kZThreads, 3)
+    k_yz_inv(const __grid_constant__ CUtensorMap tmap, typename Cplx<T>::type *specD, T *__restrict__ out,
+             const PassArgs<T> a, const FuseArgs fa) {
+  using C = typename Cplx<T>::type;
+  constexpr int W = 128 / sizeof(C);
+  extern __shared__ unsigned char smraw[];
+  __shared__ int s_ticket;
+  __shared__ __align__(8) uint64_t mbar;
+  C *sm = reinterpret_cast<C *>(align128(smraw));
+  const int ny = NY > 0 ? NY : a.nj;
+  const int total = fa.planes * (fa.prod_pp + fa.cons_pp);
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+  }
+  uint32_t loads = 0;   // completed phases of mbar
+  for (;;) {
+    const int t = next_ticket(fa.ticket, &s_ticket);
+    if (t >= total) break;
+    bool cons;
+    int plane, tile;
+    fuse_decode(fa, t, cons, plane, tile);
+    if (!cons) {
+      // y inverse of a tile of the x pass's output (written by an earlier
+      // launch, so TMA may read it)
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (!tma_tile<C, W, false>(&tmap, sm, &mbar, loads & 1, ny, fa.box_rows, plane, tile, a.status)) break;
+      loads++;
+      PointTile<W, C> tl{sm};
+      y_tile<T, W, true, NY>(tl, specD, a, plane, tile, sm);
+      publish(fa.done, plane);
+    } else {
+      if (!await_plane(fa, plane, a.status)) break;
+      const long first = (long)plane * a.nj;
+      z_inv_tile<T, NZ, false>(specD, out, a, fa.zW, fa.zP, first + (long)tile * 2 * fa.zW, first + a.nj, sm,
+                               ZTileIO{nullptr, 0, a.status});
+    }
+  }
+}
+
+// x pass: forward, filter, inverse; one TMA-loaded tile per block.
+template <typename T, int N>
+static void launch_x(const CUtensorMap &map, typename Cplx<T>::type *dst, const PassArgs<T> &a, int box_rows,
+                     int grid, size_t smem, cudaStream_t st) {
+  constexpr int W = 128 / (2 * (int)sizeof(T));
+  k_strided<T, W, true, false, N><<<grid, kZThreads, smem, st>>>(map, dst, a, box_rows);
 }
 
 // ------------------------------------------------------------- plan tables
@@ -314,14 +664,22 @@ using namespace ff;
 
 namespace ff {
 
-// Launch shape of a persistent strided pass.
+// Launch shape of a strided pass (one TMA tile per block).
 struct StridedCfg {
   int N;          // specialised length of the kernel, 0 = runtime plan
-  int threads;    // block size
   int W;          // columns per tile
   int box_rows;   // rows per TMA box (a divisor of n, at most 256)
   size_t smem;    // dynamic shared memory: one tile + alignment slack
   int grid;       // one block per tile
+};
+
+// Launch shape of a fused persistent pass.
+struct FusedCfg {
+  int NZ, NY;     // specialised z and y lengths of the kernel (0 = runtime plan)
+  size_t smem;
+  int grid;
+  int lag;
+  int prod_pp, cons_pp;
 };
 
 }  // namespace ff
@@ -339,12 +697,15 @@ struct ff_plan {
   AxisDev<float2> axf[3];
   double *kk[3];
   int *status;
+  int *counters;       // fused passes: 2 tickets + 2 x ni plane counts
+  int fused;           // 1: three launches (fused z/y passes), 0: five launches
   int zN;              // z passes: specialised length, 0 = runtime plan
   int zW, zP;          // z passes: line pairs per block, line pitch in complex values
   size_t zsmem;
   unsigned ztiles;
   StridedCfg ycfg, xcfg;
-  cudaEvent_t ev[FF_NUM_PHASES + 1];
+  FusedCfg fwd, inv;
+  cudaEvent_t ev[FF_MAX_PHASES + 1];
 };
 
 namespace ff {
@@ -403,11 +764,15 @@ template <typename F> static int allow_dyn_smem(F fn, size_t *avail) {
   return FF_OK;
 }
 
-template <typename T>
-using StridedKernel = void (*)(const CUtensorMap, typename Cplx<T>::type *, const PassArgs<T>, int);
 template <typename T> using ZFwdKernel = void (*)(const T *, typename Cplx<T>::type *, const PassArgs<T>, int, int);
 template <typename T>
 using ZInvKernel = void (*)(const typename Cplx<T>::type *, T *, const PassArgs<T>, int, int);
+template <typename T>
+using StridedKernel = void (*)(const CUtensorMap, typename Cplx<T>::type *, const PassArgs<T>, int);
+template <typename T>
+using FwdKernel = void (*)(const T *, typename Cplx<T>::type *, const PassArgs<T>, const FuseArgs);
+template <typename T>
+using InvKernel = void (*)(const CUtensorMap, typename Cplx<T>::type *, T *, const PassArgs<T>, const FuseArgs);
 
 // The specialised length for an axis of n points, or 0 (runtime plan).
 static int special_n(int n) {
@@ -431,17 +796,39 @@ template <typename T> static ZInvKernel<T> zinv_kernel(int N) {
 }
 
 // kind: 0 = y forward, 1 = y inverse, 2 = x (forward, filter, inverse);
-// 128-byte rows (W = 8 FP64 / 16 FP32), 256 threads.
+// 128-byte rows (W = 8 FP64 / 16 FP32).
 template <typename T, int N> static StridedKernel<T> strided_n(int kind) {
   constexpr int W = 128 / (2 * (int)sizeof(T));
-  return kind == 0 ? k_strided<T, W, false, false, 256, N>
-                   : kind == 1 ? k_strided<T, W, false, true, 256, N> : k_strided<T, W, true, false, 256, N>;
+  return kind == 0 ? k_strided<T, W, false, false, N>
+                   : kind == 1 ? k_strided<T, W, false, true, N> : k_strided<T, W, true, false, N>;
 }
 template <typename T> static StridedKernel<T> strided_kernel(int kind, int N) {
 #define FF_CASE(NN) if (N == NN) return strided_n<T, NN>(kind);
   FF_FOR_EACH_SPECIAL_N(FF_CASE)
 #undef FF_CASE
   return strided_n<T, 0>(kind);
+}
+
+// (z, y) length pairs with specialised fused kernels; others use (0, 0).
+#define FF_FOR_EACH_FUSED_PAIR(X) X(512, 512) X(256, 512) X(256, 256) X(1024, 1024)
+
+static void fused_pair(int nk, int nj, int *NZ, int *NY) {
+  *NZ = *NY = 0;
+#define FF_CASE(A, B) if (nk == A && nj == B) { *NZ = A; *NY = B; }
+  FF_FOR_EACH_FUSED_PAIR(FF_CASE)
+#undef FF_CASE
+}
+template <typename T> static FwdKernel<T> fwd_kernel(int NZ, int NY) {
+#define FF_CASE(A, B) if (NZ == A && NY == B) return k_zy_fwd<T, A, B>;
+  FF_FOR_EACH_FUSED_PAIR(FF_CASE)
+#undef FF_CASE
+  return k_zy_fwd<T, 0, 0>;
+}
+template <typename T> static InvKernel<T> inv_kernel(int NZ, int NY) {
+#define FF_CASE(A, B) if (NZ == A && NY == B) return k_yz_inv<T, A, B>;
+  FF_FOR_EACH_FUSED_PAIR(FF_CASE)
+#undef FF_CASE
+  return k_yz_inv<T, 0, 0>;
 }
 
 // Largest divisor d of n with d <= cap and d % step == 0 (0 if none).
@@ -454,36 +841,71 @@ static int largest_divisor_at_most(int n, int cap, int step) {
 template <typename T> static int configure(ff_plan *p) {
   using C = typename Cplx<T>::type;
   const size_t csz = sizeof(C);
-  // z passes: W line pairs, two line-major buffers of pitch P, ~64 KB per block
+  const int ni = p->n[0], nj = p->n[1], nk = p->n[2];
+  // z tiles: W line pairs, two line-major buffers of pitch P, ~64 KB per block
   const int align = csz == 16 ? 8 : 16;
-  p->zN = special_n(p->n[2]);
-  p->zP = (p->n[2] + align - 1) / align * align;
+  p->zN = special_n(nk);
+  p->zP = (nk + align - 1) / align * align;
   const size_t per_pair = 2 * (size_t)p->zP * csz;
   p->zW = (int)std::max<size_t>(1, std::min<size_t>(8, (64 * 1024) / per_pair));
-  p->zsmem = p->zW * per_pair;
-  const long npairs = ((long)p->n[0] * p->n[1] + 1) / 2;
+  // A: max(W*P, 2W*nhp) values (stages, then output staging), B: W*P values
+  // (+ slack for a copy rounded up to 16 bytes), base alignment
+  const size_t a_bytes = (std::max<size_t>((size_t)p->zW * p->zP, 2 * (size_t)p->zW * p->nhp) * csz + 127) & ~size_t(127);
+  p->zsmem = a_bytes + (size_t)p->zW * p->zP * csz + 128 + 128;
+  const long npairs = ((long)ni * nj + 1) / 2;
   p->ztiles = (unsigned)((npairs + p->zW - 1) / p->zW);
   int rc = allow_dyn_smem(zfwd_kernel<T>(p->zN), nullptr);
   if (rc == FF_OK) rc = allow_dyn_smem(zinv_kernel<T>(p->zN), nullptr);
   if (rc != FF_OK) return rc;
-  // strided passes: one tile of W 128-byte columns x n rows per block
+  // strided tiles: W 128-byte columns x n rows, one per block
   const int W = 128 / (int)csz;
+  const int ktiles = (p->nh + W - 1) / W;
   for (int kind = 0; kind < 3; kind++) {
     StridedCfg &cfg = kind == 2 ? p->xcfg : p->ycfg;
-    const int n = kind == 2 ? p->n[0] : p->n[1];
+    const int n = kind == 2 ? ni : nj;
     cfg.N = special_n(n);
-    cfg.threads = 256;
     cfg.W = W;
     cfg.box_rows = largest_divisor_at_most(n, 256, 1);
     cfg.smem = (size_t)n * W * csz + 128;
-    StridedKernel<T> fn = strided_kernel<T>(kind, cfg.N);
     size_t avail = 0;
-    rc = allow_dyn_smem(fn, &avail);
+    rc = allow_dyn_smem(strided_kernel<T>(kind, cfg.N), &avail);
     if (rc != FF_OK) return rc;
     if (cfg.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "no tile shape for an axis of %d points", n);
-    const long ktiles = (p->nh + W - 1) / W;
-    cfg.grid = (int)((kind == 2 ? p->n[1] : p->n[0]) * ktiles);
+    cfg.grid = (kind == 2 ? nj : ni) * ktiles;
   }
+  // fused passes: persistent blocks over the in-order tile queue
+  const int zpp = (nj + 2 * p->zW - 1) / (2 * p->zW);   // z tiles per plane (pairs never cross planes)
+  for (int dir = 0; dir < 2; dir++) {
+    FusedCfg &fc = dir == 0 ? p->fwd : p->inv;
+    fused_pair(nk, nj, &fc.NZ, &fc.NY);
+    fc.smem = std::max(p->zsmem, p->ycfg.smem);
+    fc.prod_pp = dir == 0 ? zpp : ktiles;
+    fc.cons_pp = dir == 0 ? ktiles : zpp;
+    int per_sm = 0;
+    size_t avail = 0;
+    if (dir == 0) {
+      FwdKernel<T> fn = fwd_kernel<T>(fc.NZ, fc.NY);
+      rc = allow_dyn_smem(fn, &avail);
+      if (rc != FF_OK) return rc;
+      if (fc.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "fused pass does not fit (%zu bytes)", fc.smem);
+      FF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kZThreads, fc.smem));
+    } else {
+      InvKernel<T> fn = inv_kernel<T>(fc.NZ, fc.NY);
+      rc = allow_dyn_smem(fn, &avail);
+      if (rc != FF_OK) return rc;
+      if (fc.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "fused pass does not fit (%zu bytes)", fc.smem);
+      FF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kZThreads, fc.smem));
+    }
+    if (per_sm < 1) return set_error(FF_ERR_UNSUPPORTED, "fused pass does not fit on an SM");
+    const long total = (long)ni * (fc.prod_pp + fc.cons_pp);
+    fc.grid = (int)std::min<long>(total, (long)per_sm * p->num_sms);
+    // consumers of plane i are queued once the blocks in flight have moved
+    // about 1.5 grids of tiles past its producers
+    const int per_plane = fc.prod_pp + fc.cons_pp;
+    fc.lag = std::min(ni, std::max(2, (3 * fc.grid + 2 * per_plane - 1) / (2 * per_plane)));
+  }
+  const char *mode = getenv("FF_PASSES");
+  p->fused = mode && strcmp(mode, "3") == 0;
   return FF_OK;
 }
 
@@ -555,27 +977,45 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
   int rc = spectrum_map<T>(p, potential, p->ycfg, false, &ymapP);
   if (rc == FF_OK) rc = spectrum_map<T>(p, potential, p->xcfg, true, &xmapP);
   if (rc != FF_OK) return rc;
-  if (timed) FF_CUDA(cudaEventRecord(p->ev[0], st));
+  int ev = 0;
+  if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  if (p->fused) {
+    const int ni = p->n[0];
+    FF_CUDA(cudaMemsetAsync(p->counters, 0, (2 + 2 * (size_t)ni) * sizeof(int), st));
+    FuseArgs ff{p->counters, p->counters + 2, ni, p->fwd.prod_pp, p->fwd.cons_pp, p->fwd.lag, p->zW, p->zP,
+                p->ycfg.box_rows};
+    fwd_kernel<T>(p->fwd.NZ, p->fwd.NY)<<<p->fwd.grid, kZThreads, p->fwd.smem, st>>>(D, Ps, a, ff);
+    FF_CUDA(cudaGetLastError());
+    if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+    strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
+    FF_CUDA(cudaGetLastError());
+    if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+    FuseArgs fi{p->counters + 1, p->counters + 2 + ni, ni, p->inv.prod_pp, p->inv.cons_pp, p->inv.lag, p->zW, p->zP,
+                p->ycfg.box_rows};
+    inv_kernel<T>(p->inv.NZ, p->inv.NY)<<<p->inv.grid, kZThreads, p->inv.smem, st>>>(ymapP, Ds, P, a, fi);
+    FF_CUDA(cudaGetLastError());
+    if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+    return FF_OK;
+  }
   zfwd_kernel<T>(p->zN)<<<p->ztiles, kZThreads, p->zsmem, st>>>(D, Ps, a, p->zW, p->zP);
   FF_CUDA(cudaGetLastError());
-  if (timed) FF_CUDA(cudaEventRecord(p->ev[1], st));
-  strided_kernel<T>(0, p->ycfg.N)<<<p->ycfg.grid, p->ycfg.threads, p->ycfg.smem, st>>>(ymapP, Ps, a,
-                                                                                       p->ycfg.box_rows);
+  if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  strided_kernel<T>(0, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ps, a, p->ycfg.box_rows);
   FF_CUDA(cudaGetLastError());
-  if (timed) FF_CUDA(cudaEventRecord(p->ev[2], st));
-  strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, p->xcfg.threads, p->xcfg.smem, st>>>(xmapP, Ps, a,
-                                                                                       p->xcfg.box_rows);
+  if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
   FF_CUDA(cudaGetLastError());
-  if (timed) FF_CUDA(cudaEventRecord(p->ev[3], st));
-  strided_kernel<T>(1, p->ycfg.N)<<<p->ycfg.grid, p->ycfg.threads, p->ycfg.smem, st>>>(ymapP, Ds, a,
-                                                                                       p->ycfg.box_rows);
+  if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  strided_kernel<T>(1, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ds, a, p->ycfg.box_rows);
   FF_CUDA(cudaGetLastError());
-  if (timed) FF_CUDA(cudaEventRecord(p->ev[4], st));
+  if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
   zinv_kernel<T>(p->zN)<<<p->ztiles, kZThreads, p->zsmem, st>>>(Ds, P, a, p->zW, p->zP);
   FF_CUDA(cudaGetLastError());
-  if (timed) FF_CUDA(cudaEventRecord(p->ev[5], st));
+  if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
   return FF_OK;
 }
+
+static int plan_phases(const ff_plan *p) { return p->fused ? 3 : 5; }
 
 // Reads and clears the device status word; FF_ERR_TIMEOUT if a bounded wait
 // inside a kernel gave up.
@@ -586,7 +1026,10 @@ static int take_device_status(const ff_plan *p, cudaStream_t st) {
   if (h != kDevOk) {
     FF_CUDA(cudaMemsetAsync(p->status, 0, sizeof(int), st));
     FF_CUDA(cudaStreamSynchronize(st));
-    return set_error(FF_ERR_TIMEOUT, "a TMA tile load did not complete within its wait limit (device status %d)", h);
+    return set_error(FF_ERR_TIMEOUT, "%s (device status %d)",
+                     h == kDevTmaTimeout ? "a TMA tile load did not complete within its wait limit"
+                                         : "a fused pass waited too long for a plane's producer tiles",
+                     h);
   }
   return FF_OK;
 }
@@ -613,13 +1056,18 @@ const char *ff_status_string(int s) {
   }
 }
 
-const char *ff_phase_name(int p) {
-  // phase names of the reference's stamps (ParisPencil.cpp:142-424) that
-  // survive on one GPU, one per pass
-  static const char *names[FF_NUM_PHASES] = {"Real-to-complex FFT in Z", "Forward FFT in Y", "X FFTs and filter",
-                                             "Backward FFT in Y", "Complex-to-real FFT in Z"};
-  return (p >= 0 && p < FF_NUM_PHASES) ? names[p] : "";
+const char *ff_phase_name(const ff_plan *p, int q) {
+  // the reference's stamp names (ParisPencil.cpp:142-424) for the phases that
+  // survive on one GPU; the fused passes join two of them
+  static const char *five[5] = {"Real-to-complex FFT in Z", "Forward FFT in Y", "X FFTs and filter",
+                                "Backward FFT in Y", "Complex-to-real FFT in Z"};
+  static const char *three[3] = {"Real-to-complex FFT in Z + Forward FFT in Y", "X FFTs and filter",
+                                 "Backward FFT in Y + Complex-to-real FFT in Z"};
+  if (!p || q < 0 || q >= plan_phases(p)) return "";
+  return p->fused ? three[q] : five[q];
 }
+
+int ff_plan_phases(const ff_plan *p) { return p ? plan_phases(p) : 0; }
 
 int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int precision, ff_plan **out) {
   if (!n || !lo || !hi || !out) return set_error(FF_ERR_INVALID, "ff_plan_create: null argument");
@@ -676,7 +1124,8 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
     o_kk[d] = take((d == 2 ? p->nh : n[d]) * sizeof(double));
   }
   const size_t o_status = take(sizeof(int));
-  for (int e = 0; e <= FF_NUM_PHASES; e++) {
+  const size_t o_counters = take((2 + 2 * (size_t)n[0]) * sizeof(int));
+  for (int e = 0; e <= FF_MAX_PHASES; e++) {
     if (cudaEventCreate(&p->ev[e]) != cudaSuccess) {
       for (int q = 0; q < e; q++) cudaEventDestroy(p->ev[q]);
       delete p;
@@ -685,12 +1134,13 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
   }
   if (cudaMalloc(&p->dmem, off) != cudaSuccess) {
     cudaGetLastError();
-    for (int e = 0; e <= FF_NUM_PHASES; e++) cudaEventDestroy(p->ev[e]);
+    for (int e = 0; e <= FF_MAX_PHASES; e++) cudaEventDestroy(p->ev[e]);
     delete p;
     return set_error(FF_ERR_NOMEM, "ff_plan_create: cudaMalloc(%zu) for plan tables failed", off);
   }
   char *base = static_cast<char *>(p->dmem);
   p->status = reinterpret_cast<int *>(base + o_status);
+  p->counters = reinterpret_cast<int *>(base + o_counters);
   int rc = FF_OK;
   if (cudaMemset(p->status, 0, sizeof(int)) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_plan_create: memset");
   for (int d = 0; d < 3 && rc == FF_OK; d++) {
@@ -758,14 +1208,16 @@ int ff_solve(const ff_plan *p, size_t bytes, void *density, void *potential, voi
                                    : launch_solve<float>(p, density, potential, st, timed);
   if (rc != FF_OK) return rc;
   if (timed) {
-    FF_CUDA(cudaEventSynchronize(p->ev[FF_NUM_PHASES]));
-    for (int q = 0; q < FF_NUM_PHASES; q++) {
+    const int np = plan_phases(p);
+    FF_CUDA(cudaEventSynchronize(p->ev[np]));
+    times->count = np;
+    for (int q = 0; q < FF_MAX_PHASES; q++) {
       float ms = 0;
-      FF_CUDA(cudaEventElapsedTime(&ms, p->ev[q], p->ev[q + 1]));
+      if (q < np) FF_CUDA(cudaEventElapsedTime(&ms, p->ev[q], p->ev[q + 1]));
       times->ms[q] = ms;
     }
     float tot = 0;
-    FF_CUDA(cudaEventElapsedTime(&tot, p->ev[0], p->ev[FF_NUM_PHASES]));
+    FF_CUDA(cudaEventElapsedTime(&tot, p->ev[0], p->ev[np]));
     times->total_ms = tot;
     return take_device_status(p, st);
   }
@@ -780,7 +1232,7 @@ int ff_plan_check(const ff_plan *p, void *stream) {
 int ff_plan_destroy(ff_plan *p) {
   if (!p) return FF_OK;
   int rc = FF_OK;
-  for (int e = 0; e <= FF_NUM_PHASES; e++)
+  for (int e = 0; e <= FF_MAX_PHASES; e++)
     if (p->ev[e]) cudaEventDestroy(p->ev[e]);
   if (p->dmem && cudaFree(p->dmem) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_plan_destroy: cudaFree failed");
   delete p;

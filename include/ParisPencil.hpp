@@ -51,9 +51,9 @@ class ParisPencil {
     ff_phase_times times;
     check(ff_solve(plan_, bytes, density, potential, nullptr, &times), __LINE__);
     double t = t0;
-    for (int p = 0; p < FF_NUM_PHASES; p++) {
+    for (int p = 0; p < times.count; p++) {
       t += 1e-3 * times.ms[p];
-      stamps.push_back({ff_phase_name(p), t});
+      stamps.push_back({ff_phase_name(plan_, p), t});
     }
   }
 

@@ -57,15 +57,14 @@ typedef struct {
   double a, theta;
 } ff_mode;
 
-/* Per-pass device times of one solve, in milliseconds (CUDA events). */
-#define FF_NUM_PHASES 5
+/* Per-launch device times of one solve, in milliseconds (CUDA events):
+ * count = ff_plan_phases(plan) entries of ms are filled. */
+#define FF_MAX_PHASES 5
 typedef struct {
-  double ms[FF_NUM_PHASES];
+  int count;
+  double ms[FF_MAX_PHASES];
   double total_ms;
 } ff_phase_times;
-
-/* Name of phase p (0..FF_NUM_PHASES-1), e.g. "Real-to-complex FFT in Z". */
-const char *ff_phase_name(int p);
 
 /* Plan a solve of an n[0] x n[1] x n[2] periodic grid (x slowest, z fastest:
  * index (i*n[1]+j)*n[2]+k).  lo/hi are the physical bounds with hi one cell
@@ -82,6 +81,13 @@ int ff_plan_bytes(const ff_plan *plan, size_t *bytes);
 
 /* Grid dimensions and precision of a plan. */
 int ff_plan_info(const ff_plan *plan, int n[3], int *precision);
+
+/* Number of device launches (phases) of a solve: 5, one per pass (the
+ * default), or 3 with the z and y passes fused through L2 (environment
+ * FF_PASSES=3 at plan creation).  Name of phase q, built from the reference's stamp names
+ * (ParisPencil.cpp:142-424), e.g. "X FFTs and filter". */
+int ff_plan_phases(const ff_plan *plan);
+const char *ff_phase_name(const ff_plan *plan, int q);
 
 /* Solve lap(phi) = f.  density: device array holding f (FP64 or FP32 per the
  * plan), at least ff_plan_bytes() bytes; it is used as a work array and

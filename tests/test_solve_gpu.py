@@ -149,8 +149,10 @@ def test_paris_pencil_drop_in(torch_cuda, ff, oracle):
     f = d[:N].cpu().numpy().reshape(n)
     stamps = []
     pp.solve(nb, d, p, stamps)
-    assert stamps[0][0] == "Total" and len(stamps) == 1 + ff.FF_NUM_PHASES
-    assert [s[0] for s in stamps[1:]] == ff.phase_names()
+    names = ff.phase_names(pp)
+    assert stamps[0][0] == "Total" and len(stamps) == 1 + len(names)
+    assert [s[0] for s in stamps[1:]] == names
+    assert "X FFTs and filter" in names
     assert stamps[-1][1] >= stamps[0][1]
     assert rel_l2(p[:N].cpu().numpy().reshape(n), oracle.solve(f)) <= FP64_TOL
 
@@ -182,7 +184,7 @@ def test_fishfry_driver_printout(ff):
     for r_ in runs:
         assert max(float(x) for x in r_[3:]) < 1e-14
     assert "Times Averaged across Iterations" in out
-    for name in ["Total"] + ff.phase_names():
+    for name in ["Total", "X FFTs and filter"]:
         assert re.search(r"\(\s*[\d.]+%\) \| " + re.escape(name) + "$", out, re.M)
 
 
@@ -251,3 +253,19 @@ def test_parity_with_reference_binary(torch_cuda, ff, n, tmp_path):
     plan.solve(d, p)
     phi = p[:N].cpu().numpy().reshape(n)
     assert rel_l2(phi, phi_ref) <= FP64_TOL
+
+
+@pytest.mark.parametrize("n", [(64, 64, 64), (30, 45, 50), (512, 16, 24), (16, 512, 512)])
+def test_fused_passes_parity(torch_cuda, ff, oracle, n, monkeypatch):
+    """Three-launch mode (z and y passes fused through L2, FF_PASSES=3) gives
+    the same phi as the oracle."""
+    monkeypatch.setenv("FF_PASSES", "3")
+    plan = ff.Plan(n)
+    assert plan.phases() == 3
+    d = torch_cuda.empty(plan.nbytes // 8, dtype=torch_cuda.float64, device="cuda")
+    p = torch_cuda.empty_like(d)
+    ff.init_field(n, d)
+    N = n[0] * n[1] * n[2]
+    f = d[:N].cpu().numpy().reshape(n)
+    plan.solve(d, p, timed=True)
+    assert rel_l2(p[:N].cpu().numpy().reshape(n), oracle.solve(f)) <= FP64_TOL
