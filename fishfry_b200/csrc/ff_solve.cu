@@ -117,7 +117,7 @@ __device__ __forceinline__ void bulk_out(E *dst, const E *src, size_t count) {
 // order into B; the split A[k] = (Z[k] + conj Z[n-k]) / 2,
 // B[k] = (Z[k] - conj Z[n-k]) / (2i) goes out with consecutive threads on
 // consecutive k.
-template <typename T, int N, bool TMAIO>
+template <typename T, int N, bool TMAIO, bool TMA_OUT = TMAIO>
 __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cplx<T>::type *spec, const PassArgs<T> &a,
                                            int W, int P, long line0, long lend, typename Cplx<T>::type *sm,
                                            const ZTileIO &io) {
@@ -138,7 +138,7 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
       const int la = 2 * c;
       return mk(la < nl ? raw[la * nk + pos] : (T)0, la + 1 < nl ? raw[(la + 1) * nk + pos] : (T)0);
     };
-    dif_all<N, false, Map::PosFast, 1, kZThreads, true, false>(ax, ld0, tA, tBrev, W);
+    dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ld0, tA, tBrev, W);
     // split into the staging rows [line][kh] (pitch nhp) in A, then one copy out
     const T h = (T)0.5;
     for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
@@ -161,17 +161,32 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
       if (la + 1 < lend) y = f[(la + 1) * nk + pos];
       return mk(x, y);
     };
-    dif_all<N, false, Map::PosFast, 1, kZThreads, true, false>(ax, ldg, tA, tBrev, W);
+    dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ldg, tA, tBrev, W);
     const T h = (T)0.5;
-    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-      const int k = it % nh;
-      const int c = it / nh;
-      const long la = line0 + 2 * c;
-      if (la >= lend) continue;
-      const C z = tB(k, c);
-      const C w = tB(k == 0 ? 0 : nk - k, c);
-      spec[la * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
-      if (la + 1 < lend) spec[(la + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+    if constexpr (TMA_OUT) {
+      // staged rows [line][kh] (pitch nhp) in A, then one copy out
+      for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+        const int k = it % nh;
+        const int c = it / nh;
+        const C z = tB(k, c);
+        const C w = tB(k == 0 ? 0 : nk - k, c);
+        A[(2 * c) * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
+        A[(2 * c + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+      }
+      fence_proxy_async_smem();
+      __syncthreads();
+      bulk_out(spec + line0 * a.nhp, A, (size_t)nl * a.nhp);
+    } else {
+      for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+        const int k = it % nh;
+        const int c = it / nh;
+        const long la = line0 + 2 * c;
+        if (la >= lend) continue;
+        const C z = tB(k, c);
+        const C w = tB(k == 0 ? 0 : nk - k, c);
+        spec[la * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
+        if (la + 1 < lend) spec[(la + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+      }
     }
     return true;
   }
@@ -214,7 +229,7 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
       hermitian(k, c, sa, sb);
     }
     __syncthreads();
-    dif_all<N, true, Map::PosFast, 1, kZThreads, true, false>(ax, tB, tA, tBrev, W);
+    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, tB, tA, tBrev, W);
     // real lines staged in A, then one copy out
     T *raw = reinterpret_cast<T *>(A);
     for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
@@ -239,7 +254,7 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
       hermitian(k, c, sa, sb);
     }
     __syncthreads();
-    dif_all<N, true, Map::PosFast, 1, kZThreads, true, false>(ax, tB, tA, tBrev, W);
+    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, tB, tA, tBrev, W);
     for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
       const int t = it % nk;
       const int c = it / nk;
@@ -411,9 +426,10 @@ __device__ __forceinline__ unsigned char *align128(unsigned char *p) {
 
 // ------------------------------------------------- unfused pass kernels
 // (one launch per pass; used when the fused passes are switched off)
-// Specialised lengths move their z tiles with bulk copies (their line blocks
-// are always 16-byte aligned and have at least two stages); other lengths
-// read and write HBM from the threads.
+// For specialised lengths (line blocks always 16-byte aligned, at least two
+// stages) the forward z pass reads its lines from the threads (coalesced) and
+// writes its spectrum rows with one bulk copy, and the inverse moves its line
+// blocks both ways with bulk copies; other lengths use the threads for both.
 template <typename T, int N>
 __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, typename Cplx<T>::type *spec,
                                                        const PassArgs<T> a, int W, int P) {
@@ -426,7 +442,7 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, 
   __syncthreads();
   const long nlines = (long)a.ni * a.nj;
   const ZTileIO io{&mbar, 0, a.status};
-  z_fwd_tile<T, N, (N > 0)>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+  z_fwd_tile<T, N, false, (N > 0)>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                             reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
 
