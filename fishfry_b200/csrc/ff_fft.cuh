@@ -7,9 +7,9 @@
 //     touches whole rows and every access is bank-conflict free.  Used by the
 //     strided passes (y and x), whose global rows are W contiguous columns.
 //   * line-major   sm[c*P + swz(pos)]: each line contiguous (pitch P), with an
-//     XOR swizzle of the 16-byte chunk inside every 128-byte row so unit-,
-//     8- and 64-element strides are all conflict free.  Used by the z passes,
-//     whose global lines are contiguous; threads take positions fastest.
+//     XOR swizzle of the element inside every 128-byte row so power-of-two
+//     strides are conflict free.  Used by the z passes, whose global lines
+//     are contiguous; threads take positions fastest.
 //
 // Transforms are in-place mixed-radix Cooley-Tukey:
 //   * decimation in frequency (DIF): natural input, output at position pos
@@ -246,13 +246,15 @@ enum class Map { ColFast, PosFast };
 //   ncols: columns in the tile (must be W for Map::ColFast).
 //   NC, LC > 0: compile-time length and span (NC = 0: use n_rt, L_rt);
 //   NT > 0: compile-time block size; with NC it fully unrolls the item loop.
-template <int R, bool INV, bool DIT, Map MAP, int W, int NT, int NC, int LC, bool TWREC, typename C, typename LD,
-          typename ST>
+//   TWMUL: the twiddle table is TWMUL times longer than n (a sub-transform of
+//   a longer line uses that line's table).
+template <int R, bool INV, bool DIT, Map MAP, int W, int NT, int NC, int LC, bool TWREC, int TWMUL = 1, typename C,
+          typename LD, typename ST>
 __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, LD &ld, ST &st, int ncols) {
   const int n = NC ? NC : n_rt;
   const int L = NC ? LC : L_rt;
   const int m = L / R;
-  const int twstep = n / L;
+  const int twstep = TWMUL * n / L;
   const int nb = n / R;
   auto body = [&](int it) {
     int c, b;
@@ -311,11 +313,14 @@ template <int W, typename C> struct PointTile {
   __device__ __forceinline__ void operator()(int pos, int c, C v) const { sm[pos * W + c] = v; }
 };
 
-// Line-major swizzled tile: element (pos, c) at sm[c*P + swz(pos)]; the 16-byte
-// chunk index inside each 128-byte row is XORed with the row index mod 8.
+// Line-major swizzled tile: element (pos, c) at sm[c*P + swz(pos)]; the
+// element index inside each 128-byte row is XORed with the row index (mod 8
+// for 16-byte FP64 elements, mod 16 for 8-byte FP32 elements).  Shared memory
+// serves 16-byte accesses per quarter warp and 8-byte ones per half warp, so
+// unit, 2-, 4-, 8- and row-strided position sets are all conflict free.
 // P must be a multiple of 8 (FP64) or 16 (FP32) elements.
 __device__ __forceinline__ int swz(int pos, double2 *) { return pos ^ ((pos >> 3) & 7); }
-__device__ __forceinline__ int swz(int pos, float2 *) { return pos ^ (((pos >> 4) & 7) << 1); }
+__device__ __forceinline__ int swz(int pos, float2 *) { return pos ^ ((pos >> 4) & 15); }
 
 template <typename C> struct LineTile {
   C *sm;
@@ -404,32 +409,34 @@ __device__ __forceinline__ void dit_rt(const AxisDev<C> &ax, int s_begin, MID &m
 
 // Compile-time plan of length N: DIF stages s..SEND-1 as dif_rt does.
 // TWREC0: recurrence twiddles in stage 0; TWALL: in every stage.
-template <int N, int SEND, int s, bool INV, Map MAP, int W, int NT, bool TWREC0, bool TWALL, typename C,
-          typename LD0, typename MID, typename STL>
+// TWMUL: the axis table is TWMUL times longer than N (N is a sub-transform).
+template <int N, int SEND, int s, bool INV, Map MAP, int W, int NT, bool TWREC0, bool TWALL, int TWMUL = 1,
+          typename C, typename LD0, typename MID, typename STL>
 __device__ __forceinline__ void dif_ct(const AxisDev<C> &ax, LD0 &ld0, MID &mid, STL &stl, int ncols) {
   if constexpr (s < SEND) {
     constexpr int R = plan_radix(N, s);
     constexpr int L = plan_span(N, s);
     constexpr bool TWR = TWALL || (TWREC0 && s == 0);
-    if constexpr (s == 0 && SEND == 1) stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, ld0, stl, ncols);
-    else if constexpr (s == 0) stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, ld0, mid, ncols);
-    else if constexpr (s == SEND - 1) stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, mid, stl, ncols);
-    else stage<R, INV, false, MAP, W, NT, N, L, TWR>(N, L, ax, mid, mid, ncols);
+    if constexpr (s == 0 && SEND == 1) stage<R, INV, false, MAP, W, NT, N, L, TWR, TWMUL>(N, L, ax, ld0, stl, ncols);
+    else if constexpr (s == 0) stage<R, INV, false, MAP, W, NT, N, L, TWR, TWMUL>(N, L, ax, ld0, mid, ncols);
+    else if constexpr (s == SEND - 1) stage<R, INV, false, MAP, W, NT, N, L, TWR, TWMUL>(N, L, ax, mid, stl, ncols);
+    else stage<R, INV, false, MAP, W, NT, N, L, TWR, TWMUL>(N, L, ax, mid, mid, ncols);
     __syncthreads();
-    dif_ct<N, SEND, s + 1, INV, MAP, W, NT, TWREC0, TWALL>(ax, ld0, mid, stl, ncols);
+    dif_ct<N, SEND, s + 1, INV, MAP, W, NT, TWREC0, TWALL, TWMUL>(ax, ld0, mid, stl, ncols);
   }
 }
 
 // Compile-time plan of length N: DIT stages s..0 as dit_rt does.
-template <int N, int s, bool INV, Map MAP, int W, int NT, bool TWALL, typename C, typename MID, typename STL>
+template <int N, int s, bool INV, Map MAP, int W, int NT, bool TWALL, int TWMUL = 1, typename C, typename MID,
+          typename STL>
 __device__ __forceinline__ void dit_ct(const AxisDev<C> &ax, MID &mid, STL &stl, int ncols) {
   if constexpr (s >= 0) {
     constexpr int R = plan_radix(N, s);
     constexpr int L = plan_span(N, s);
-    if constexpr (s == 0) stage<R, INV, true, MAP, W, NT, N, L, TWALL>(N, L, ax, mid, stl, ncols);
-    else stage<R, INV, true, MAP, W, NT, N, L, TWALL>(N, L, ax, mid, mid, ncols);
+    if constexpr (s == 0) stage<R, INV, true, MAP, W, NT, N, L, TWALL, TWMUL>(N, L, ax, mid, stl, ncols);
+    else stage<R, INV, true, MAP, W, NT, N, L, TWALL, TWMUL>(N, L, ax, mid, mid, ncols);
     __syncthreads();
-    dit_ct<N, s - 1, INV, MAP, W, NT, TWALL>(ax, mid, stl, ncols);
+    dit_ct<N, s - 1, INV, MAP, W, NT, TWALL, TWMUL>(ax, mid, stl, ncols);
   }
 }
 

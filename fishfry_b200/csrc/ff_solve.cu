@@ -17,6 +17,7 @@
 // The reference's 12 reorder kernels and 6 MPI_Alltoall self-copies reduce to
 // the choice of row stride in passes 2-4.
 
+#include <cooperative_groups.h>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -337,6 +338,9 @@ __device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T
                                        typename Cplx<T>::type *sm) {
   using C = typename Cplx<T>::type;
   constexpr int NT = kZThreads;
+  // FP64: twiddle powers by recurrence (fewer table loads); FP32: table loads
+  // (FP64-generated values), keeping the FP64 pipe for the filter
+  constexpr bool TWX = sizeof(T) == 8;
   const AxisDev<C> &ax = a.ax[0];
   const int n = N > 0 ? N : ax.n;
   const int kh0 = kt * W;
@@ -365,10 +369,10 @@ __device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T
     constexpr int S = plan_stages(N);
     constexpr int RF = plan_radix(N, S - 1);
     if constexpr (S > 1) {
-      dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, true>(ax, tile, tile, tile, W);
+      dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, TWX>(ax, tile, tile, tile, W);
       fused_filter_stage<RF, W, NT, N, C>(N, tile, tile, filt);
       __syncthreads();
-      dit_ct<N, S - 2, true, Map::ColFast, W, NT, true>(ax, tile, gst, W);
+      dit_ct<N, S - 2, true, Map::ColFast, W, NT, TWX>(ax, tile, gst, W);
     } else {
       fused_filter_stage<RF, W, NT, N, C>(N, tile, gst, filt);
     }
@@ -487,6 +491,152 @@ __global__ void __launch_bounds__(kZThreads, 3)
   } else {
     PointTile<W, C> tile{sm};
     y_tile<T, W, INV, N>(tile, dst, a, o, kt, sm);
+  }
+}
+
+// ------------------------------------------- long lines on a CTA pair
+// A strided tile of N = 2H rows (N = 1024) would need 128 KB of shared
+// memory and a whole SM.  Instead a 2-block cluster holds it, block r keeping
+// rows [r*H, r*H + H) (64 KB, 128-byte rows, three blocks per SM).  The plan
+// is radix 2 first: the span-N radix-2 stage pairs row j of block 0 with row
+// j of block 1 and runs over distributed shared memory; what is left on each
+// block is an independent H-point transform (the compile-time plan of H,
+// twiddles from the N table), whose output frequency is k = r + 2*rev_H(pos).
+// The x pass mirrors it: H-point stages, filter, H-point inverse stages, and
+// the span-N radix-2 DIT stage across the pair last.
+
+// Cross-block radix-2 stage of span 2H on rows j of `lo` (block 0) and `hi`
+// (block 1); block r takes j in [r*H/2, (r+1)*H/2), so every pair of
+// locations belongs to one item (read and written in place).
+// The items are taken in batches of B whose loads (half of them from the
+// partner block) are all issued before any store.
+template <bool INV, bool DIT, int W, int H, typename C>
+__device__ __forceinline__ void pair_stage(C *lo, C *hi, int r, const AxisDev<C> &ax) {
+  constexpr int ITEMS = W * (H / 2);
+  constexpr int Q = ITEMS / kZThreads;
+  constexpr int B = 4;
+  static_assert(ITEMS % kZThreads == 0 && Q % B == 0, "pair stage shape");
+#pragma unroll 1
+  for (int q0 = 0; q0 < Q; q0 += B) {
+    C v0[B], v1[B];
+    int at[B], jj[B];
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      const int it = (int)threadIdx.x + (q0 + b) * kZThreads;
+      const int c = it % W;
+      jj[b] = r * (H / 2) + it / W;
+      at[b] = jj[b] * W + c;
+      v0[b] = lo[at[b]];
+      v1[b] = hi[at[b]];
+    }
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+      C v[2] = {v0[b], v1[b]};
+      if (DIT) {
+        if (jj[b]) v[1] = twmul<INV>(v[1], ax.tw, jj[b]);
+        Dft<2, INV, C>::run(v);
+      } else {
+        Dft<2, INV, C>::run(v);
+        if (jj[b]) v[1] = twmul<INV>(v[1], ax.tw, jj[b]);
+      }
+      lo[at[b]] = v[0];
+      hi[at[b]] = v[1];
+    }
+  }
+}
+
+template <typename T, bool XPASS, bool INV, int N>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kZThreads, 3)
+    k_strided_pair(const __grid_constant__ CUtensorMap tmap, typename Cplx<T>::type *dst, const PassArgs<T> a,
+                   int box_rows) {
+  using C = typename Cplx<T>::type;
+  namespace cg = cooperative_groups;
+  constexpr int W = 128 / sizeof(C);
+  constexpr int H = N / 2;
+  constexpr int NT = kZThreads;
+  extern __shared__ unsigned char smraw[];
+  __shared__ __align__(8) uint64_t mbar;
+  cg::cluster_group cl = cg::this_cluster();
+  const int r = (int)cl.block_rank();
+  C *sm = reinterpret_cast<C *>(align128(smraw));
+  const AxisDev<C> &ax = XPASS ? a.ax[0] : a.ax[1];
+  const int ktiles = (a.nh + W - 1) / W;
+  const int tile = blockIdx.x / 2;
+  const int o = tile / ktiles, kt = tile - o * ktiles;
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_init_fence();
+    mbar_expect_tx(&mbar, (uint32_t)(H * W * sizeof(C)));
+    for (int q = 0; q < H / box_rows; q++) {
+      if (XPASS) tma_load_3d(sm + q * box_rows * W, &tmap, 2 * W * kt, o, r * H + q * box_rows, &mbar);
+      else tma_load_3d(sm + q * box_rows * W, &tmap, 2 * W * kt, r * H + q * box_rows, o, &mbar);
+    }
+  }
+  __syncthreads();
+  bool ok = mbar_wait_bounded(&mbar, 0);
+  ok = !__syncthreads_or(!ok);
+  if (!ok && threadIdx.x == 0) {
+    // report; the block still takes part in every cluster barrier below (its
+    // partner must not wait forever), but skips the work
+    atomicExch(a.status, kDevTmaTimeout);
+    mbar_wait_bounded(&mbar, 0);
+  }
+  cl.sync();   // both halves resident
+  C *peer = cl.map_shared_rank(sm, r ^ 1);
+  C *lo = r == 0 ? sm : peer;
+  C *hi = r == 0 ? peer : sm;
+  if (ok) pair_stage<INV && !XPASS, false, W, H>(lo, hi, r, ax);
+  cl.sync();   // the rest is local to each block
+  const int kh0 = kt * W;
+  const int ncol = min(W, a.nh - kh0);
+  PointTile<W, C> tile_{sm};
+  if (!XPASS) {
+    if (ok) {
+      const long base = (long)o * a.nj * a.nhp + kh0;
+      const int pitch = a.nhp;
+      auto gst = [&](int pos, int c, C v) {
+        if (c < ncol) dst[base + (long)(r + 2 * rev_ct<H>(pos)) * pitch + c] = v;
+      };
+      dif_ct<H, plan_stages(H), 0, INV, Map::ColFast, W, NT, false, false, 2>(ax, tile_, tile_, gst, W);
+    }
+    return;
+  }
+  constexpr int S = plan_stages(H);
+  constexpr int RF = plan_radix(H, S - 1);
+  const int j = o;
+  const int ni = a.ni;
+  const double jd = double(min(j, a.nj - j)) * a.dd[1];
+  const double j2 = jd * jd;
+  const double ddi = a.dd[0], ddk = a.dd[2];
+  const double minvN = -a.invN;
+  // d = -1/((i2 + j2) + k2) as ParisPencil.cpp:276-279 forms it, times 1/N
+  auto filt = [&](int pos, int c, C v) -> C {
+    const int kx = r + 2 * rev_ct<H>(pos);
+    const int kh = kh0 + c;
+    if (c >= ncol) return v;
+    if ((kx | j | kh) == 0) return mk((T)0, (T)0);
+    const double id = double(min(kx, ni - kx)) * ddi;
+    const double kd = double(kh) * ddk;
+    const double d = recip_pos((id * id + j2) + kd * kd) * minvN;
+    return cscale(v, (T)d);
+  };
+  if (ok) {
+    dif_ct<H, S - 1, 0, false, Map::ColFast, W, NT, false, (sizeof(T) == 8), 2>(ax, tile_, tile_, tile_, W);
+    fused_filter_stage<RF, W, NT, H, C>(H, tile_, tile_, filt);
+    __syncthreads();
+    dit_ct<H, S - 2, true, Map::ColFast, W, NT, (sizeof(T) == 8), 2>(ax, tile_, tile_, W);
+  }
+  cl.sync();
+  if (ok) pair_stage<true, true, W, H>(lo, hi, r, ax);
+  cl.sync();   // both halves final; no remote access after this
+  if (!ok) return;
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < H / box_rows; q++)
+      tma_store_3d(&tmap, 2 * W * kt, j, r * H + q * box_rows, sm + q * box_rows * W);
+    bulk_commit();
+    bulk_wait_read();
   }
 }
 
@@ -819,6 +969,9 @@ template <typename T, int N> static StridedKernel<T> strided_n(int kind) {
                    : kind == 1 ? k_strided<T, W, false, true, N> : k_strided<T, W, true, false, N>;
 }
 template <typename T> static StridedKernel<T> strided_kernel(int kind, int N) {
+  if (N == 1024)   // one tile per 2-block cluster
+    return kind == 0 ? k_strided_pair<T, false, false, 1024>
+                     : kind == 1 ? k_strided_pair<T, false, true, 1024> : k_strided_pair<T, true, false, 1024>;
 #define FF_CASE(NN) if (N == NN) return strided_n<T, NN>(kind);
   FF_FOR_EACH_SPECIAL_N(FF_CASE)
 #undef FF_CASE
@@ -882,12 +1035,13 @@ template <typename T> static int configure(ff_plan *p) {
     cfg.N = special_n(n);
     cfg.W = W;
     cfg.box_rows = largest_divisor_at_most(n, 256, 1);
-    cfg.smem = (size_t)n * W * csz + 128;
+    const int pair = cfg.N == 1024 ? 2 : 1;   // tile rows split over a 2-block cluster
+    cfg.smem = (size_t)(n / pair) * W * csz + 128;
     size_t avail = 0;
     rc = allow_dyn_smem(strided_kernel<T>(kind, cfg.N), &avail);
     if (rc != FF_OK) return rc;
     if (cfg.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "no tile shape for an axis of %d points", n);
-    cfg.grid = (kind == 2 ? nj : ni) * ktiles;
+    cfg.grid = (kind == 2 ? nj : ni) * ktiles * pair;
   }
   // fused passes: persistent blocks over the in-order tile queue
   const int zpp = (nj + 2 * p->zW - 1) / (2 * p->zW);   // z tiles per plane (pairs never cross planes)
@@ -921,7 +1075,8 @@ template <typename T> static int configure(ff_plan *p) {
     fc.lag = std::min(ni, std::max(2, (3 * fc.grid + 2 * per_plane - 1) / (2 * per_plane)));
   }
   const char *mode = getenv("FF_PASSES");
-  p->fused = mode && strcmp(mode, "3") == 0;
+  // the fused passes hold a whole y tile per block: not for 1024-point y lines
+  p->fused = mode && strcmp(mode, "3") == 0 && p->ycfg.N != 1024;
   return FF_OK;
 }
 

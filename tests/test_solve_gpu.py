@@ -46,7 +46,8 @@ def rel_l2(a, b):
 PARITY_SIZES = [(8, 8, 8), (16, 16, 16), (12, 10, 8), (5, 9, 6), (2, 3, 5), (1, 4, 6), (3, 1, 1), (1, 1, 2),
                 (30, 45, 50), (64, 48, 40), (64, 64, 64), (100, 36, 27), (96, 80, 75), (128, 128, 128),
                 (45, 81, 125), (256, 96, 72), (1800, 2, 4), (4, 1800, 6), (6, 5, 1800), (243, 16, 10),
-                (1024, 8, 10), (6, 960, 9), (1215, 4, 6), (3, 1125, 4), (1125, 3, 1215)]
+                (1024, 8, 10), (6, 960, 9), (1215, 4, 6), (3, 1125, 4), (1125, 3, 1215), (4, 1024, 6),
+                (1024, 1024, 2), (30, 1024, 1024)]
 
 
 @pytest.mark.parametrize("n", PARITY_SIZES)
@@ -157,7 +158,7 @@ def test_paris_pencil_drop_in(torch_cuda, ff, oracle):
     assert rel_l2(p[:N].cpu().numpy().reshape(n), oracle.solve(f)) <= FP64_TOL
 
 
-@pytest.mark.parametrize("n", [(64, 64, 64), (128, 96, 80), (30, 45, 50)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 96, 80), (30, 45, 50), (1024, 24, 20), (16, 1024, 64)])
 def test_fp32_precision_form(torch_cuda, ff, oracle, n):
     modes = ff.modes_generate(12345, 64, 32, ff.alias_free_kaxis(n))
     f64 = oracle.init_f(n, modes)
