@@ -32,13 +32,22 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 L2_BYTES = 126 * 1024 * 1024
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, bytes per
+# launch) of each pass, from one `ncu --set full` capture of each kernel of
+# `fishfry_b200/bin/fishfry 1 1 1 512 512 512 1`; the capture's summary is
+# profiles/passes_fp64_512cube_ncu_full.txt.
+MEASURED_TRAFFIC = {
+    ("512x512x512", "fp64"): {
+        "Real-to-complex FFT in Z": 2.104563e9, "Forward FFT in Y": 2.102818e9, "X FFTs and filter": 2.102127e9,
+        "Backward FFT in Y": 2.104016e9, "Complex-to-real FFT in Z": 2.104495e9,
+    },
+}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--grid", type=int, nargs=3, default=[512, 512, 512])
@@ -64,50 +73,90 @@ def bytes_model(n, precision, launches=3):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clocks and clock-event (throttle) reasons sampled every few ms by
+    NVML while the timed region runs; nvidia-smi at 200 ms when the NVML
+    bindings are missing."""
 
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
-        self.index = index
-        self.rows = []
-        self.proc = None
+    def __init__(self, device, period_s=0.005):
+        self.device = device
+        self.period = period_s
+        self.rows = []          # (sm_mhz, max_mhz, reason bitmask)
+        self.stop_flag = threading.Event()
         self.thread = None
+        self.proc = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        prop = torch.cuda.get_device_properties(self.device)
+        try:
+            bus = "%08x:%02x:%02x.0" % (prop.pci_domain_id, prop.pci_bus_id, prop.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except OSError:
-            self.proc = None
-            return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+            nv, h = self._nvml_handle()
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception:
+            return self._start_smi()
+        self.source = "nvml"
+
+        def loop():
+            while not self.stop_flag.is_set():
+                try:
+                    self.rows.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx, int(reasons(h))))
+                except Exception:
+                    pass
+                time.sleep(self.period)
+        self.thread = threading.Thread(target=loop, daemon=True)
         self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) == 7:
-                self.rows.append(parts)
+    def _start_smi(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            return
+        self.source = "nvidia-smi"
+
+        def read():
+            for line in self.proc.stdout:
+                r = [x.strip() for x in line.split(",")]
+                if len(r) == 7 and r[0].replace(".", "").isdigit():
+                    bits = sum(b for q, (_, b) in enumerate(self.REASON_BITS) if r[3 + q].lower().startswith("active"))
+                    self.rows.append((float(r[0]), float(r[1]), bits))
+        self.thread = threading.Thread(target=read, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        if self.source is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"], "samples": 0}
+        self.stop_flag.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
         self.thread.join(timeout=5)
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[q] for r in self.rows for q in range(4) if r[3 + q].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        rows = list(self.rows)
+        reasons = sorted({name for _, _, bits in rows for name, b in self.REASON_BITS if bits & b})
+        return {"sm_mhz": statistics.median(r[0] for r in rows) if rows else None,
+                "sm_max_mhz": max(r[1] for r in rows) if rows else None, "reasons": reasons,
+                "samples": len(rows), "source": self.source}
 
 
 def cpu_info():
@@ -276,13 +325,7 @@ def run_ours(args):
         peak_src = "measured" if peak else "fallback"
         peak = peak or 6650.0
         achieved = per_pass_bytes[top] / (pass_ms[top] * 1e-3) / 1e9
-        traffic = None
-        try:
-            tr = json.load(open(PROFILE_TRAFFIC))
-            key = "%dx%dx%d_%s" % (*n, args.precision)
-            traffic = tr.get(key, {}).get(names[top])
-        except (OSError, ValueError):
-            pass
+        traffic = MEASURED_TRAFFIC.get(("%dx%dx%d" % n, args.precision), {}).get(names[top])
         solve_gbs = total_bytes / (ms_per_step * 1e-3) / 1e9
         five_gbs = five_pass_bytes / (ms_per_step * 1e-3) / 1e9
         cpu = None

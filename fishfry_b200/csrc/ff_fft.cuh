@@ -269,17 +269,55 @@ __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, 
     const int j = b - blk * m;
     const int base = blk * L + j;
     C v[R];
+    // Compile-time stage with twiddles: the factors are fetched before the
+    // data loads and applied without a branch (j = 0 reads exp(0) = 1), so
+    // their latency overlaps the data loads.  Not for FP64 line-major tiles,
+    // where the extra live registers spill.
+    constexpr bool kPrefetch = !(MAP == Map::PosFast && sizeof(C) == 16);
+    if constexpr (NC > 0 && LC > R && R > 1 && kPrefetch) {
+      if constexpr (TWREC) {
+        double2 w1 = __ldg(ax.tw64 + j * twstep);
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = ld(base + r * m, c);
-    if (DIT) {
-      if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
-      Dft<R, INV, C>::run(v);
+        for (int r = 0; r < R; r++) v[r] = ld(base + r * m, c);
+        if (INV) w1.y = -w1.y;
+        auto apply = [&] {
+          double2 w = w1;
+#pragma unroll
+          for (int r = 1; r < R; r++) {
+            v[r] = cmul(v[r], to_c(w, (C *)nullptr));
+            if (r + 1 < R) w = cmul(w, w1);
+          }
+        };
+        if (DIT) { apply(); Dft<R, INV, C>::run(v); }
+        else { Dft<R, INV, C>::run(v); apply(); }
+      } else {
+        C w[R - 1];
+#pragma unroll
+        for (int r = 1; r < R; r++) w[r - 1] = __ldg(ax.tw + j * r * twstep);
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = ld(base + r * m, c);
+        auto apply = [&] {
+#pragma unroll
+          for (int r = 1; r < R; r++) v[r] = INV ? cmulc(v[r], w[r - 1]) : cmul(v[r], w[r - 1]);
+        };
+        if (DIT) { apply(); Dft<R, INV, C>::run(v); }
+        else { Dft<R, INV, C>::run(v); apply(); }
+      }
+#pragma unroll
+      for (int r = 0; r < R; r++) st(base + r * m, c, v[r]);
     } else {
-      Dft<R, INV, C>::run(v);
-      if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
-    }
 #pragma unroll
-    for (int r = 0; r < R; r++) st(base + r * m, c, v[r]);
+      for (int r = 0; r < R; r++) v[r] = ld(base + r * m, c);
+      if (DIT) {
+        if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
+        Dft<R, INV, C>::run(v);
+      } else {
+        Dft<R, INV, C>::run(v);
+        if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
+      }
+#pragma unroll
+      for (int r = 0; r < R; r++) st(base + r * m, c, v[r]);
+    }
   };
   if constexpr (NC > 0 && NT > 0 && MAP == Map::ColFast && (W * (NC / R)) % NT == 0) {
     constexpr int ITER = W * (NC / R) / NT;
@@ -525,6 +563,12 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 // Waits until every committed bulk store of this thread has finished reading
 // shared memory (the buffer may then be reused or released).
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+// L2 prefetch hint of a contiguous range (16-byte aligned, size a multiple of
+// 16).  No data reaches shared memory and no completion is tracked.
+__device__ __forceinline__ void l2_prefetch(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
 
 // Device-side status word values (plan status buffer).
 enum : int { kDevOk = 0, kDevTmaTimeout = 1, kDevDepTimeout = 2 };

@@ -40,6 +40,7 @@ template <typename T> struct PassArgs {
   double invN;             // 1 / (ni*nj*nk)
   double dd[3];            // wavenumber scales (ParisPencil.cpp:9-11)
   int *status;             // device status word (kDev*), 0 = ok
+  int l2_ahead;            // forward z pass: block b prefetches block b + l2_ahead's lines into L2 (0: off)
 };
 
 constexpr int kZThreads = 256;
@@ -290,7 +291,7 @@ __device__ __forceinline__ void y_tile(LD0 &ld0, typename Cplx<T>::type *dst, co
   auto gst = [&](int pos, int c, C v) {
     if (c < ncol) dst[base + (long)rl(pos) * pitch + c] = v;
   };
-  dif_all<N, INV, Map::ColFast, W, kZThreads, false, false>(ax, ld0, tile, gst, W);
+    dif_all<N, INV, Map::ColFast, W, kZThreads, false, (sizeof(T) == 8)>(ax, ld0, tile, gst, W);
 }
 
 // The last DIF stage of the x forward transform, the filter and the first
@@ -445,6 +446,12 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, 
   }
   __syncthreads();
   const long nlines = (long)a.ni * a.nj;
+  if (N > 0 && threadIdx.x == 0) {
+    // whole lines of a specialised length are 16-byte multiples
+    const long fl = ((long)blockIdx.x + a.l2_ahead) * (2 * W);
+    if (a.l2_ahead > 0 && fl < nlines)
+      l2_prefetch(f + fl * a.nk, (uint32_t)(min((long)(2 * W), nlines - fl) * a.nk * sizeof(T)));
+  }
   const ZTileIO io{&mbar, 0, a.status};
   z_fwd_tile<T, N, false, (N > 0)>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                             reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
@@ -869,6 +876,7 @@ struct ff_plan {
   int zW, zP;          // z passes: line pairs per block, line pitch in complex values
   size_t zsmem;
   unsigned ztiles;
+  int l2_ahead;        // forward z pass: L2 prefetch distance in blocks (0: off)
   StridedCfg ycfg, xcfg;
   FusedCfg fwd, inv;
   cudaEvent_t ev[FF_MAX_PHASES + 1];
@@ -1074,6 +1082,13 @@ template <typename T> static int configure(ff_plan *p) {
     const int per_plane = fc.prod_pp + fc.cons_pp;
     fc.lag = std::min(ni, std::max(2, (3 * fc.grid + 2 * per_plane - 1) / (2 * per_plane)));
   }
+  // The forward z pass runs one tile per block, three blocks per SM, each
+  // waiting on its thread-issued line loads.  Block b hints block
+  // b + l2_ahead's lines into L2, so that read is under way while the
+  // resident blocks compute and lands as L2 hits.  (The same hint slows the
+  // TMA-fed passes.)
+  const char *ahead = getenv("FF_L2_AHEAD");
+  p->l2_ahead = ahead ? std::max(0, atoi(ahead)) : 3 * p->num_sms;
   const char *mode = getenv("FF_PASSES");
   // the fused passes hold a whole y tile per block: not for 1024-point y lines
   p->fused = mode && strcmp(mode, "3") == 0 && p->ycfg.N != 1024;
@@ -1133,6 +1148,7 @@ template <typename T> static PassArgs<T> pass_args(const ff_plan *p) {
   a.invN = 1.0 / (double(p->n[0]) * double(p->n[1]) * double(p->n[2]));
   for (int d = 0; d < 3; d++) a.dd[d] = p->dd[d];
   a.status = p->status;
+  a.l2_ahead = p->l2_ahead;
   return a;
 }
 
