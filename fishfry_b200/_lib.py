@@ -29,6 +29,8 @@ EXPORTS = [
     "ff_plan_destroy",
     "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_status_string",
     "ff_last_error", "ff_version",
+    "ff_batch_create", "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
+    "ff_batch_destroy",
 ]
 
 
@@ -74,8 +76,19 @@ def _declare(L):
     L.ff_status_string.restype = ctypes.c_char_p
     L.ff_last_error.restype = ctypes.c_char_p
     L.ff_version.restype = ctypes.c_char_p
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.ff_batch_create.argtypes = [ctypes.c_int, ip, d3, d3, ctypes.c_int, ctypes.POINTER(vp)]
+    L.ff_batch_bytes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+    L.ff_batch_solve.argtypes = [vp, pp, pp, vp, ctypes.POINTER(PhaseTimes)]
+    L.ff_batch_tune.argtypes = [vp, pp, pp, vp, ctypes.c_int]
+    L.ff_batch_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
+    L.ff_batch_check.argtypes = [vp, vp]
+    L.ff_batch_destroy.argtypes = [vp]
     for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
-                 "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate"):
+                 "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_batch_create",
+                 "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
+                 "ff_batch_destroy"):
         getattr(L, name).restype = ctypes.c_int
 
 

@@ -96,6 +96,75 @@ class Plan:
             pass
 
 
+class Batch:
+    """Many independent grids solved together: five persistent launches (one
+    per pass) over the tiles of all grids, captured once in a CUDA graph.
+
+    dims: list of (ni, nj, nk); lo/hi: per-grid bounds or None for the
+    reference domain of each grid.
+    """
+
+    def __init__(self, dims, precision=FF_FP64, lo=None, hi=None):
+        dims = [tuple(int(x) for x in d) for d in dims]
+        cnt = len(dims)
+        flat = (ctypes.c_int * (3 * cnt))(*[x for d in dims for x in d])
+        lo_a = hi_a = None
+        if lo is not None:
+            lo_a = (ctypes.c_double * (3 * cnt))(*[float(x) for v in lo for x in v])
+            hi_a = (ctypes.c_double * (3 * cnt))(*[float(x) for v in hi for x in v])
+        h = ctypes.c_void_p()
+        check(lib().ff_batch_create(cnt, flat, lo_a, hi_a, int(precision), ctypes.byref(h)), "ff_batch_create")
+        self._h = h
+        self.dims = dims
+        self.precision = int(precision)
+        self.nbytes = []
+        for g in range(cnt):
+            b = ctypes.c_size_t()
+            check(lib().ff_batch_bytes(h, g, ctypes.byref(b)), "ff_batch_bytes")
+            self.nbytes.append(b.value)
+
+    def __len__(self):
+        return len(self.dims)
+
+    @staticmethod
+    def _ptrs(bufs):
+        return (ctypes.c_void_p * len(bufs))(*[_ptr(b) for b in bufs])
+
+    def solve(self, density, potential, stream=None, timed=False):
+        """Enqueue the batch solve; with timed, waits and returns (per-pass ms, total ms)."""
+        times = _lib.PhaseTimes() if timed else None
+        self._keep = (self._ptrs(density), self._ptrs(potential))
+        check(lib().ff_batch_solve(self._h, self._keep[0], self._keep[1], _stream(stream),
+                                   ctypes.byref(times) if timed else None), "ff_batch_solve")
+        if timed:
+            return list(times.ms)[:times.count], times.total_ms
+        return None
+
+    def tune(self, density, potential, stream=None, reps=3):
+        """Autotune the tile shapes (overwrites the buffers)."""
+        d, p = self._ptrs(density), self._ptrs(potential)
+        check(lib().ff_batch_tune(self._h, d, p, _stream(stream), int(reps)), "ff_batch_tune")
+
+    def shape(self, index, kind):
+        W, ct = ctypes.c_int(), ctypes.c_int()
+        check(lib().ff_batch_shape(self._h, int(index), int(kind), ctypes.byref(W), ctypes.byref(ct)), "ff_batch_shape")
+        return W.value, ct.value
+
+    def check(self, stream=None):
+        check(lib().ff_batch_check(self._h, _stream(stream)), "ff_batch_check")
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            check(lib().ff_batch_destroy(self._h), "ff_batch_destroy")
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class ParisPencil:
     """The reference plugin interface (ParisPencil.hpp:11-59) on one GPU.
 

@@ -20,8 +20,8 @@ BIN = os.path.join(HERE, "bin", "fishfry")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
 
-LIB_SOURCES = ["ff_solve.cu", "ff_field.cu"]
-HEADERS = ["ff_fft.cuh", "ff_status.hpp"]
+LIB_SOURCES = ["ff_solve.cu", "ff_field.cu", "ff_batch.cu", "ff_batch_f64.cu", "ff_batch_f32.cu"]
+HEADERS = ["ff_fft.cuh", "ff_tiles.cuh", "ff_status.hpp", "ff_batch.hpp", "ff_batch_dev.cuh"]
 
 
 def _nvcc():
@@ -53,11 +53,12 @@ def build_lib(verbose=False, force=False):
     if not force and not _stale(LIB, deps):
         return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    objs = []
-    for s in srcs:
-        o = os.path.join(HERE, "lib", os.path.basename(s) + ".o")
-        _run([_nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o], verbose)
-        objs.append(o)
+    objs = [os.path.join(HERE, "lib", os.path.basename(s) + ".o") for s in srcs]
+    # translation units compile in parallel (each is one nvcc process)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(_run, [_nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o], verbose) for s, o in zip(srcs, objs)]:
+            f.result()
     tmp = LIB + ".tmp"
     _run([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"], verbose)
     os.replace(tmp, LIB)

@@ -1,0 +1,555 @@
+// The batched form: many independent grids of uneven sizes solved by five
+// persistent launches (one per pass) captured once in a CUDA graph, with
+// tile shapes picked by a measuring autotuner.  Each grid's solve is the
+// single-grid algorithm (ParisPencil.cpp:95-425 restated as five passes).
+//
+// Host side: axis tables shared by all grids of one length, the grid
+// descriptors, the per-pass work lists (prefix sums of tiles over grids), the
+// graph, and the tuner.  The kernels are in ff_batch_dev.cuh.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "ff_batch.hpp"
+#include "ff_status.hpp"
+#include "ff_tiles.cuh"
+
+namespace ff {
+
+// Shared with the single-grid plan (ff_solve.cu).
+std::vector<int> plan_factor_radices(int n);
+std::vector<int> plan_digit_reversal(int n, const std::vector<int> &radix);
+
+namespace {
+
+struct AxisSlot {
+  int n;
+  size_t o_tw, o_tw64, o_rev, o_ipos;
+};
+
+// Tuned shapes, process-wide: (precision, pass kind, axis length) -> shape.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, TileShape> g_tuned;
+
+int axis_of_kind(int kind) { return kind == 0 || kind == 4 ? 2 : kind == 2 ? 0 : 1; }
+
+}  // namespace
+}  // namespace ff
+
+using namespace ff;
+
+struct ff_batch {
+  int count = 0;
+  int precision = FF_FP64;
+  int device = 0;
+  int num_sms = 0;
+  size_t csz = 16;
+  std::vector<BatchGridHost> grids;
+  std::vector<size_t> bytes;
+  void *dmem = nullptr;          // axis tables, status, tickets, descriptors, work lists
+  size_t dmem_size = 0;
+  std::vector<AxisSlot> axes;
+  int *status = nullptr;
+  int *tickets = nullptr;        // one per pass
+  void *desc = nullptr;          // device grid descriptors
+  size_t desc_size = 0;
+  unsigned char *desc_host = nullptr;   // pinned image of the descriptors
+  int2 *entries[5] = {};
+  int *starts[5] = {};
+  int ntiles[5] = {};
+  int blocks[5] = {};
+  size_t smem[5] = {};
+  bool desc_dirty = true;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[6] = {};
+};
+
+namespace ff {
+namespace {
+
+size_t desc_size(int precision) {
+  return precision == FF_FP64 ? batch_desc_size<double>() : batch_desc_size<float>();
+}
+
+void desc_fill(int precision, void *dst, const BatchGridHost &g) {
+  if (precision == FF_FP64) batch_desc_fill<double>(dst, g);
+  else batch_desc_fill<float>(dst, g);
+}
+
+int pass_prepare(int precision, int kind, size_t smem, int *per_sm) {
+  return precision == FF_FP64 ? batch_pass_prepare<double>(kind, smem, per_sm)
+                              : batch_pass_prepare<float>(kind, smem, per_sm);
+}
+
+int pass_launch(const ff_batch *b, int kind, cudaStream_t st) {
+  const BatchWork wl{b->entries[kind], b->starts[kind], b->count, b->tickets + kind};
+  return b->precision == FF_FP64 ? batch_pass_launch<double>(kind, b->desc, wl, b->blocks[kind], b->smem[kind], st)
+                                 : batch_pass_launch<float>(kind, b->desc, wl, b->blocks[kind], b->smem[kind], st);
+}
+
+int axis_len(const BatchGridHost &g, int kind) { return g.n[axis_of_kind(kind)]; }
+
+// Tiles of one pass of one grid.
+int tiles_of(const BatchGridHost &g, int kind) {
+  const TileShape &s = g.shape[kind];
+  if (kind == 0 || kind == 4) {
+    const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
+    return (int)((npairs + s.W - 1) / s.W);
+  }
+  const long ncols = (long)(kind == 2 ? g.n[1] : g.n[0]) * g.nh;
+  return (int)((ncols + s.W - 1) / s.W);
+}
+
+size_t shape_smem(const ff_batch *b, const BatchGridHost &g, int kind, const TileShape &s) {
+  return batch_tile_smem(kind, axis_len(g, kind), g.n[2], g.nhp, s.W, b->csz);
+}
+
+bool shape_valid(const ff_batch *b, const BatchGridHost &g, int kind, const TileShape &s) {
+  if (s.W < 1) return false;
+  if (s.ct && !batch_special_n(axis_len(g, kind))) return false;
+  if (kind != 0 && kind != 4) {
+    const int w1 = 128 / (int)b->csz;
+    if (s.W != w1 && s.W != 2 * w1 && s.W != 4 * w1) return false;
+  }
+  return shape_smem(b, g, kind, s) <= kBatchSmem;
+}
+
+// Default shape: about 256 butterfly items per stage (one per thread) within
+// the shared-memory budget; compile-time tiles where the length has them.
+TileShape default_shape(const ff_batch *b, const BatchGridHost &g, int kind) {
+  const int n = axis_len(g, kind);
+  TileShape s{1, batch_special_n(n) ? 1 : 0};
+  if (kind == 0 || kind == 4) {
+    const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
+    int W = std::max(1, 2048 / std::max(1, g.n[2]));
+    W = (int)std::min<long>(W, npairs);
+    while (W > 1 && !shape_valid(b, g, kind, TileShape{W, s.ct})) W--;
+    s.W = W;
+    return s;
+  }
+  const int w1 = 128 / (int)b->csz;
+  int W = w1;
+  for (int m = 4; m >= 1; m /= 2) {
+    const TileShape t{m * w1, s.ct};
+    if (m * w1 * n <= 2048 * 2 && shape_valid(b, g, kind, t)) {
+      W = m * w1;
+      break;
+    }
+  }
+  s.W = W;
+  return s;
+}
+
+TileShape tuned_or_default(const ff_batch *b, const BatchGridHost &g, int kind) {
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(std::make_tuple(b->precision, kind, axis_len(g, kind)));
+    if (it != g_tuned.end() && shape_valid(b, g, kind, it->second)) return it->second;
+  }
+  return default_shape(b, g, kind);
+}
+
+// Work lists, block counts and shared memory of every pass from the grids'
+// current shapes; uploads lists and descriptors (synchronously).
+int build_work(ff_batch *b) {
+  for (int k = 0; k < 5; k++) {
+    std::vector<int2> ent(b->count);
+    std::vector<int> start(b->count + 1, 0);
+    size_t smem = 256;
+    for (int g = 0; g < b->count; g++) {
+      ent[g] = make_int2(g, k);
+      start[g + 1] = start[g] + tiles_of(b->grids[g], k);
+      smem = std::max(smem, shape_smem(b, b->grids[g], k, b->grids[g].shape[k]));
+    }
+    b->ntiles[k] = start[b->count];
+    b->smem[k] = smem;
+    int per_sm = 0;
+    int rc = pass_prepare(b->precision, k, smem, &per_sm);
+    if (rc != FF_OK) return rc;
+    if (per_sm < 1) return set_error(FF_ERR_UNSUPPORTED, "batch pass %d: a tile does not fit on an SM", k);
+    b->blocks[k] = std::max(1, std::min(b->ntiles[k], per_sm * b->num_sms));
+    FF_CUDA(cudaMemcpy(b->entries[k], ent.data(), ent.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    FF_CUDA(cudaMemcpy(b->starts[k], start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  b->desc_dirty = true;
+  return FF_OK;
+}
+
+void drop_graph(ff_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+// The five passes (and a reset of the tickets, and the phase events), as
+// issued on `st`; captured once into the graph.  The events are recorded as
+// external event nodes, so the host can wait on and time them after a replay.
+int issue_passes(ff_batch *b, cudaStream_t st) {
+  FF_CUDA(cudaMemsetAsync(b->tickets, 0, 5 * sizeof(int), st));
+  FF_CUDA(cudaEventRecordWithFlags(b->ev[0], st, cudaEventRecordExternal));
+  for (int k = 0; k < 5; k++) {
+    int rc = pass_launch(b, k, st);
+    if (rc != FF_OK) return rc;
+    FF_CUDA(cudaEventRecordWithFlags(b->ev[k + 1], st, cudaEventRecordExternal));
+  }
+  return FF_OK;
+}
+
+int capture(ff_batch *b) {
+  drop_graph(b);
+  FF_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+  int rc = issue_passes(b, b->cap);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(b->cap, &g);
+  if (rc != FF_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_error(FF_ERR_CUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
+  b->graph = g;
+  FF_CUDA(cudaGraphInstantiate(&b->exec, g, 0));
+  return FF_OK;
+}
+
+// Points the descriptors at the caller's buffers; marks them for upload if
+// anything changed.
+int set_buffers(ff_batch *b, void *const *density, void *const *potential) {
+  for (int g = 0; g < b->count; g++) {
+    if (!density[g] || !potential[g]) return set_error(FF_ERR_INVALID, "ff_batch: null buffer for grid %d", g);
+    if (density[g] == potential[g]) return set_error(FF_ERR_INVALID, "ff_batch: grid %d density == potential", g);
+    if (((uintptr_t)density[g] | (uintptr_t)potential[g]) & 15)
+      return set_error(FF_ERR_INVALID, "ff_batch: grid %d buffers must be 16-byte aligned", g);
+    if (b->grids[g].density != density[g] || b->grids[g].potential != potential[g]) {
+      b->grids[g].density = density[g];
+      b->grids[g].potential = potential[g];
+      b->desc_dirty = true;
+    }
+  }
+  return FF_OK;
+}
+
+int upload_desc(ff_batch *b, cudaStream_t st) {
+  if (!b->desc_dirty) return FF_OK;
+  for (int g = 0; g < b->count; g++) desc_fill(b->precision, b->desc_host + g * b->desc_size, b->grids[g]);
+  FF_CUDA(cudaMemcpyAsync(b->desc, b->desc_host, b->count * b->desc_size, cudaMemcpyHostToDevice, st));
+  // the pinned image may be rewritten by the next call only after this copy
+  FF_CUDA(cudaStreamSynchronize(st));
+  b->desc_dirty = false;
+  return FF_OK;
+}
+
+int take_status(ff_batch *b, cudaStream_t st) {
+  int h = 0;
+  FF_CUDA(cudaMemcpyAsync(&h, b->status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FF_CUDA(cudaStreamSynchronize(st));
+  if (h != kDevOk) {
+    FF_CUDA(cudaMemsetAsync(b->status, 0, sizeof(int), st));
+    FF_CUDA(cudaStreamSynchronize(st));
+    return set_error(FF_ERR_TIMEOUT, "a batch tile's bulk copy did not complete within its wait limit");
+  }
+  return FF_OK;
+}
+
+// Median of `reps` timed launches of pass `kind` (after one warm-up).
+int time_pass(ff_batch *b, int kind, cudaStream_t st, int reps, float *ms) {
+  std::vector<float> t;
+  for (int r = 0; r <= reps; r++) {
+    FF_CUDA(cudaMemsetAsync(b->tickets + kind, 0, sizeof(int), st));
+    FF_CUDA(cudaEventRecord(b->ev[0], st));
+    int rc = pass_launch(b, kind, st);
+    if (rc != FF_OK) return rc;
+    FF_CUDA(cudaEventRecord(b->ev[1], st));
+    FF_CUDA(cudaEventSynchronize(b->ev[1]));
+    float x = 0;
+    FF_CUDA(cudaEventElapsedTime(&x, b->ev[0], b->ev[1]));
+    if (r > 0) t.push_back(x);
+  }
+  std::sort(t.begin(), t.end());
+  *ms = t[t.size() / 2];
+  return FF_OK;
+}
+
+}  // namespace
+}  // namespace ff
+
+extern "C" {
+
+int ff_batch_create(int count, const int *dims, const double *lo, const double *hi, int precision, ff_batch **out) {
+  if (!out) return set_error(FF_ERR_INVALID, "ff_batch_create: null output");
+  *out = nullptr;
+  if (count < 1 || !dims) return set_error(FF_ERR_INVALID, "ff_batch_create: count %d or dims missing", count);
+  if (precision != FF_FP64 && precision != FF_FP32)
+    return set_error(FF_ERR_INVALID, "ff_batch_create: precision %d is neither FF_FP64 nor FF_FP32", precision);
+  for (int g = 0; g < count; g++)
+    for (int d = 0; d < 3; d++) {
+      const int n = dims[3 * g + d];
+      if (n < 1) return set_error(FF_ERR_INVALID, "ff_batch_create: grid %d n[%d] = %d < 1", g, d, n);
+      if (n > FF_MAX_AXIS || !smooth235(n))
+        return set_error(FF_ERR_UNSUPPORTED, "ff_batch_create: grid %d n[%d] = %d is not 2^a 3^b 5^c <= %d", g, d,
+                         n, FF_MAX_AXIS);
+      if (lo && hi && n > 1 && !(hi[3 * g + d] > lo[3 * g + d]))
+        return set_error(FF_ERR_INVALID, "ff_batch_create: grid %d hi[%d] <= lo[%d]", g, d, d);
+      // the narrowest tile of a strided pass holds whole lines of 128-byte rows
+      if ((size_t)n * 128 + 128 > kBatchSmem)
+        return set_error(FF_ERR_UNSUPPORTED, "ff_batch_create: grid %d axis of %d points exceeds the batch tiles (%zu)",
+                         g, n, (kBatchSmem - 128) / 128);
+    }
+  ff_batch *b = new ff_batch();
+  b->count = count;
+  b->precision = precision;
+  b->csz = precision == FF_FP64 ? 16 : 8;
+  if (cudaGetDevice(&b->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess) {
+    delete b;
+    return set_error(FF_ERR_CUDA, "ff_batch_create: no current CUDA device");
+  }
+  b->desc_size = desc_size(precision);
+  // distinct axis lengths -> one table set each
+  std::map<int, int> slot_of;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+  for (int g = 0; g < count; g++)
+    for (int d = 0; d < 3; d++) {
+      const int n = dims[3 * g + d];
+      if (slot_of.count(n)) continue;
+      AxisSlot s{n, 0, 0, 0, 0};
+      s.o_tw = take(n * b->csz);
+      s.o_tw64 = precision == FF_FP64 ? s.o_tw : take(n * sizeof(double2));
+      s.o_rev = take(n * sizeof(int));
+      s.o_ipos = take(n * sizeof(int));
+      slot_of[n] = (int)b->axes.size();
+      b->axes.push_back(s);
+    }
+  const size_t o_status = take(sizeof(int));
+  const size_t o_tickets = take(5 * sizeof(int));
+  const size_t o_desc = take((size_t)count * b->desc_size);
+  size_t o_ent[5], o_start[5];
+  for (int k = 0; k < 5; k++) {
+    o_ent[k] = take((size_t)count * sizeof(int2));
+    o_start[k] = take((size_t)(count + 1) * sizeof(int));
+  }
+  b->dmem_size = off;
+  int rc = FF_OK;
+  if (cudaMalloc(&b->dmem, off) != cudaSuccess) {
+    cudaGetLastError();
+    delete b;
+    return set_error(FF_ERR_NOMEM, "ff_batch_create: cudaMalloc(%zu) for tables failed", off);
+  }
+  if (cudaMallocHost((void **)&b->desc_host, (size_t)count * b->desc_size) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(b->dmem);
+    delete b;
+    return set_error(FF_ERR_NOMEM, "ff_batch_create: pinned descriptor image");
+  }
+  char *base = static_cast<char *>(b->dmem);
+  b->status = reinterpret_cast<int *>(base + o_status);
+  b->tickets = reinterpret_cast<int *>(base + o_tickets);
+  b->desc = base + o_desc;
+  for (int k = 0; k < 5; k++) {
+    b->entries[k] = reinterpret_cast<int2 *>(base + o_ent[k]);
+    b->starts[k] = reinterpret_cast<int *>(base + o_start[k]);
+  }
+  if (cudaMemset(b->status, 0, sizeof(int)) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_create: memset");
+  // axis tables: twiddles from FP64 sincospi, digit reversal of the default plan
+  std::vector<AxisDev<double2>> axd(b->axes.size());
+  std::vector<AxisDev<float2>> axf(b->axes.size());
+  for (size_t a = 0; a < b->axes.size() && rc == FF_OK; a++) {
+    const AxisSlot &s = b->axes[a];
+    const std::vector<int> radix = plan_factor_radices(s.n);
+    const std::vector<int> rev = plan_digit_reversal(s.n, radix);
+    std::vector<int> ipos(s.n);
+    for (int q = 0; q < s.n; q++) ipos[rev[q]] = q;
+    if (cudaMemcpy(base + s.o_rev, rev.data(), s.n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(base + s.o_ipos, ipos.data(), s.n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = set_error(FF_ERR_CUDA, "ff_batch_create: table upload failed");
+    const int blocks = std::min(1024, (s.n + 255) / 256);
+    k_twiddles<<<blocks, 256>>>(s.n, reinterpret_cast<double2 *>(base + s.o_tw64));
+    if (precision == FF_FP32) k_twiddles<<<blocks, 256>>>(s.n, reinterpret_cast<float2 *>(base + s.o_tw));
+    AxisDev<double2> ad{};
+    AxisDev<float2> af{};
+    ad.n = af.n = s.n;
+    ad.nstages = af.nstages = (int)radix.size();
+    for (size_t q = 0; q < radix.size(); q++) ad.radix[q] = af.radix[q] = radix[q];
+    ad.tw = reinterpret_cast<const double2 *>(base + s.o_tw);
+    af.tw = reinterpret_cast<const float2 *>(base + s.o_tw);
+    ad.tw64 = af.tw64 = reinterpret_cast<const double2 *>(base + s.o_tw64);
+    ad.rev = af.rev = reinterpret_cast<const int *>(base + s.o_rev);
+    ad.ipos = af.ipos = reinterpret_cast<const int *>(base + s.o_ipos);
+    axd[a] = ad;
+    axf[a] = af;
+  }
+  if (rc == FF_OK && (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess))
+    rc = set_error(FF_ERR_CUDA, "ff_batch_create: table kernels failed");
+  b->grids.resize(count);
+  b->bytes.resize(count);
+  for (int g = 0; g < count && rc == FF_OK; g++) {
+    BatchGridHost &h = b->grids[g];
+    std::memset(&h, 0, sizeof(h));
+    for (int d = 0; d < 3; d++) {
+      const int n = dims[3 * g + d];
+      h.n[d] = n;
+      // ParisPencil.cpp:9-11; the reference domain [-pi, pi - 2pi/n] when no bounds are given
+      const double len = (lo && hi) ? hi[3 * g + d] - lo[3 * g + d] : 2.0 * M_PI * double(n - 1) / double(n);
+      h.dd[d] = n > 1 ? 2.0 * M_PI * double(n - 1) / (double(n) * len) : 0.0;
+      h.axd[d] = axd[slot_of[n]];
+      h.axf[d] = axf[slot_of[n]];
+    }
+    h.nh = h.n[2] / 2 + 1;
+    h.nhp = precision == FF_FP64 ? h.nh : (h.nh + 1) & ~1;
+    h.invN = 1.0 / (double(h.n[0]) * double(h.n[1]) * double(h.n[2]));
+    h.status = b->status;
+    const size_t spec = (size_t)h.n[0] * h.n[1] * h.nhp * b->csz;
+    const size_t real = (size_t)h.n[0] * h.n[1] * h.n[2] * (b->csz / 2);
+    b->bytes[g] = std::max(spec, real);
+    for (int k = 0; k < 5; k++) h.shape[k] = tuned_or_default(b, h, k);
+  }
+  if (rc == FF_OK) rc = build_work(b);
+  if (rc == FF_OK && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
+    rc = set_error(FF_ERR_CUDA, "ff_batch_create: stream");
+  for (int e = 0; e < 6 && rc == FF_OK; e++)
+    if (cudaEventCreate(&b->ev[e]) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_create: event");
+  if (rc != FF_OK) {
+    ff_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return FF_OK;
+}
+
+int ff_batch_bytes(const ff_batch *b, int index, size_t *bytes) {
+  if (!b || !bytes) return set_error(FF_ERR_INVALID, "ff_batch_bytes: null argument");
+  if (index < 0 || index >= b->count) return set_error(FF_ERR_INVALID, "ff_batch_bytes: index %d", index);
+  *bytes = b->bytes[index];
+  return FF_OK;
+}
+
+int ff_batch_shape(const ff_batch *b, int index, int kind, int *W, int *ct) {
+  if (!b || index < 0 || index >= b->count || kind < 0 || kind > 4)
+    return set_error(FF_ERR_INVALID, "ff_batch_shape: bad argument");
+  if (W) *W = b->grids[index].shape[kind].W;
+  if (ct) *ct = b->grids[index].shape[kind].ct;
+  return FF_OK;
+}
+
+int ff_batch_solve(ff_batch *b, void *const *density, void *const *potential, void *stream, ff_phase_times *times) {
+  if (!b || !density || !potential) return set_error(FF_ERR_INVALID, "ff_batch_solve: null argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc = set_buffers(b, density, potential);
+  if (rc == FF_OK) rc = upload_desc(b, st);
+  if (rc == FF_OK && !b->exec) rc = capture(b);
+  if (rc != FF_OK) return rc;
+  FF_CUDA(cudaGraphLaunch(b->exec, st));
+  if (times) {
+    FF_CUDA(cudaEventSynchronize(b->ev[5]));
+    times->count = 5;
+    for (int k = 0; k < 5; k++) {
+      float ms = 0;
+      FF_CUDA(cudaEventElapsedTime(&ms, b->ev[k], b->ev[k + 1]));
+      times->ms[k] = ms;
+    }
+    float tot = 0;
+    FF_CUDA(cudaEventElapsedTime(&tot, b->ev[0], b->ev[5]));
+    times->total_ms = tot;
+    return take_status(b, st);
+  }
+  return FF_OK;
+}
+
+int ff_batch_check(ff_batch *b, void *stream) {
+  if (!b) return set_error(FF_ERR_INVALID, "ff_batch_check: null batch");
+  return take_status(b, static_cast<cudaStream_t>(stream));
+}
+
+// Coordinate search over tile shapes: for each pass and each axis length
+// used by that pass, every valid candidate shape is applied to all grids of
+// that length and the whole pass is timed; the fastest is kept (and
+// remembered for later batches of this process).  Candidates: z passes
+// W in {d/2, d, 2d} around the default d line pairs, strided passes 1, 2 or
+// 4 rows of 128 bytes per tile row; each with the compile-time tile (where
+// the length has one) and with the runtime plan.
+int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, void *stream, int reps) {
+  if (!b || !density || !potential) return set_error(FF_ERR_INVALID, "ff_batch_tune: null argument");
+  if (reps < 1) reps = 3;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int rc = set_buffers(b, density, potential);
+  if (rc != FF_OK) return rc;
+  for (int g = 0; g < b->count; g++) {
+    FF_CUDA(cudaMemsetAsync(density[g], 0, b->bytes[g], st));
+    FF_CUDA(cudaMemsetAsync(potential[g], 0, b->bytes[g], st));
+  }
+  drop_graph(b);
+  for (int k = 0; k < 5; k++) {
+    std::vector<int> lens;
+    for (const auto &g : b->grids) lens.push_back(axis_len(g, k));
+    std::sort(lens.begin(), lens.end());
+    lens.erase(std::unique(lens.begin(), lens.end()), lens.end());
+    for (int n : lens) {
+      int first = -1;
+      for (int g = 0; g < b->count; g++)
+        if (axis_len(b->grids[g], k) == n) { first = g; break; }
+      const BatchGridHost &ref = b->grids[first];
+      std::vector<TileShape> cand;
+      const TileShape d = default_shape(b, ref, k);
+      for (int ct = batch_special_n(n) ? 1 : 0; ct >= 0; ct--) {
+        if (k == 0 || k == 4) {
+          for (int W : {std::max(1, d.W / 2), d.W, d.W * 2}) cand.push_back(TileShape{W, ct});
+        } else {
+          const int w1 = 128 / (int)b->csz;
+          for (int m : {1, 2, 4}) cand.push_back(TileShape{m * w1, ct});
+        }
+      }
+      TileShape best = ref.shape[k];
+      float best_ms = 1e30f;
+      for (const TileShape &c : cand) {
+        bool ok = true;
+        for (const auto &g : b->grids)
+          if (axis_len(g, k) == n && !shape_valid(b, g, k, c)) ok = false;
+        if (!ok) continue;
+        for (auto &g : b->grids)
+          if (axis_len(g, k) == n) g.shape[k] = c;
+        rc = build_work(b);
+        if (rc == FF_OK) rc = upload_desc(b, st);
+        float ms = 0;
+        if (rc == FF_OK) rc = time_pass(b, k, st, reps, &ms);
+        if (rc != FF_OK) return rc;
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
+      }
+      for (auto &g : b->grids)
+        if (axis_len(g, k) == n) g.shape[k] = best;
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tuned[std::make_tuple(b->precision, k, n)] = best;
+    }
+  }
+  rc = build_work(b);
+  if (rc == FF_OK) rc = upload_desc(b, st);
+  if (rc == FF_OK) rc = take_status(b, st);
+  return rc;
+}
+
+int ff_batch_destroy(ff_batch *b) {
+  if (!b) return FF_OK;
+  drop_graph(b);
+  for (int e = 0; e < 6; e++)
+    if (b->ev[e]) cudaEventDestroy(b->ev[e]);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->desc_host) cudaFreeHost(b->desc_host);
+  int rc = FF_OK;
+  if (b->dmem && cudaFree(b->dmem) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_destroy: cudaFree failed");
+  delete b;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// Many independent grids per launch: host-visible declarations shared by the
+// batch translation units (ff_batch.cu host code, ff_batch_f64.cu and
+// ff_batch_f32.cu kernels).
+//
+// A batch runs the same five passes as a single solve (z R2C, y forward,
+// x forward + filter + inverse, y inverse, z C2R), but every launch covers
+// the tiles of all its grids: one persistent kernel per pass, whose blocks
+// take tiles from a ticket counter until the work list is exhausted.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <vector_types.h>
+
+#include <algorithm>
+#include <cstddef>
+
+#include "ff_fft.cuh"
+
+namespace ff {
+
+// Per-block shared-memory budget of the batch kernels (three blocks per SM).
+constexpr size_t kBatchSmem = 72 * 1024;
+
+// Axis lengths with compile-time specialised batch tiles; others use the
+// runtime plan of their axis.
+#define FF_FOR_EACH_BATCH_N(X) X(32) X(48) X(64) X(80) X(96) X(128) X(256) X(512)
+
+inline bool batch_special_n(int n) {
+#define FF_CASE(NN) if (n == NN) return true;
+  FF_FOR_EACH_BATCH_N(FF_CASE)
+#undef FF_CASE
+  return false;
+}
+
+// One launch: tiles of entries e = 0..nentry-1 are numbered start[e] ..
+// start[e+1]-1; entry e names (grid, pass).  ticket is zeroed before the
+// launch.
+struct BatchWork {
+  const int2 *entry;
+  const int *start;
+  int nentry;
+  int *ticket;
+};
+
+// Tile shape of one pass of one grid: z passes take W line pairs per tile;
+// strided passes take W columns (W * sizeof(complex) a multiple of 128
+// bytes: 1, 2 or 4 rows of 128 bytes).  ct = 1 selects the compile-time
+// specialised tile for the axis length (batch_special_n), 0 the runtime plan.
+struct TileShape {
+  int W;
+  int ct;
+};
+
+// Shared memory of one tile (bytes, with alignment slack).
+inline size_t batch_tile_smem(int kind, int n_axis, int nk, int nhp, int W, size_t csz) {
+  if (kind == 0 || kind == 4) {
+    const int align = csz == 16 ? 8 : 16;
+    const size_t P = (size_t)(nk + align - 1) / align * align;
+    const size_t a = std::max<size_t>((size_t)W * P, 2 * (size_t)W * nhp) * csz;
+    return ((a + 127) & ~size_t(127)) + (size_t)W * P * csz + 128 + 128;
+  }
+  return (size_t)n_axis * W * csz + 128;
+}
+
+// Launches pass `kind` (0..4) of the precision-T batch kernel; grids points
+// at the device array of the batch's grid descriptors.
+template <typename T>
+int batch_pass_launch(int kind, const void *grids, const BatchWork &wl, int blocks, size_t smem, cudaStream_t st);
+// Raises the pass kernel's shared-memory limit to kBatchSmem and reports how
+// many blocks of `smem` bytes fit on one SM.
+template <typename T> int batch_pass_prepare(int kind, size_t smem, int *per_sm);
+// Size and alignment of the device grid descriptor for precision T.
+template <typename T> size_t batch_desc_size();
+// Fills the device grid descriptor image at dst (batch_desc_size bytes).
+struct BatchGridHost;
+template <typename T> void batch_desc_fill(void *dst, const BatchGridHost &g);
+
+// Host description of one grid of a batch (what batch_desc_fill packs).
+struct BatchGridHost {
+  int n[3];
+  int nh, nhp;
+  double dd[3];
+  double invN;
+  AxisDev<double2> axd[3];
+  AxisDev<float2> axf[3];
+  int *status;
+  void *density, *potential;
+  TileShape shape[5];
+};
+
+}  // namespace ff

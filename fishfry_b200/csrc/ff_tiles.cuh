@@ -1,0 +1,297 @@
+// Tile-level device code shared by the single-grid passes (ff_solve.cu) and
+// the many-grid passes (ff_batch.cu): the per-grid pass arguments, the z
+// line-pair tiles (R2C / C2R along z), the fused x filter stage and helpers.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "ff_fft.cuh"
+
+namespace ff {
+
+template <typename T> struct PassArgs {
+  using C = typename Cplx<T>::type;
+  int ni, nj, nk, nh, nhp;
+  AxisDev<C> ax[3];        // 0: x (n = ni), 1: y (nj), 2: z (nk)
+  const double *kk[3];     // (min(i, n-i) * dd)^2 per axis; kk[2] indexed by kh
+  double invN;             // 1 / (ni*nj*nk)
+  double dd[3];            // wavenumber scales (ParisPencil.cpp:9-11)
+  int *status;             // device status word (kDev*), 0 = ok
+  int l2_ahead;            // forward z pass: block b prefetches block b + l2_ahead's lines into L2 (0: off)
+};
+
+constexpr int kZThreads = 256;
+
+// Frequency of a last-stage DIF position: arithmetic for compile-time plans,
+// one table load per radix group otherwise.
+template <int N> struct RevLastOf { using type = RevCT<N>; };
+template <> struct RevLastOf<0> { using type = RevLast<0, 0>; };
+template <int N, typename C> __device__ __forceinline__ typename RevLastOf<N>::type rev_last(const AxisDev<C> &ax) {
+  if constexpr (N > 0) {
+    return RevCT<N>{};
+  } else {
+    const int R = ax.radix[ax.nstages - 1];
+    return RevLast<0, 0>{ax.rev, R, ax.n / R};
+  }
+}
+
+// ------------------------------------------------------------------ z tiles
+// A z tile is W line pairs held in two line-major buffers A, B of pitch P.
+// Pair c is lines (line0 + 2c, line0 + 2c + 1), transformed as
+// z = f[a] + i f[b]; lines at or past `lend` are absent (zero in, no output).
+//
+// With TMAIO the tile's lines enter and leave by bulk copies between HBM and
+// shared memory (the copy engine moves them; the threads only touch shared
+// memory), using the buffers as staging: the real lines land in B, the stages
+// run in A, the last stage writes B, and the output is staged in A.  Without
+// TMAIO the first stage reads HBM and the output is written from registers.
+// A holds max(W*P, 2W*nhp) complex values, B holds W*P (+ 128 bytes slack).
+struct ZTileIO {
+  uint64_t *mbar;      // TMAIO: barrier of the inbound copy
+  uint32_t parity;     // TMAIO: its phase
+  int *status;         // TMAIO: timeout report
+};
+
+// Inbound bulk copy of `bytes` (rounded up to 16) from src into dst, waited
+// for on every thread with an iteration limit.
+__device__ __forceinline__ bool bulk_in(void *dst, const void *src, size_t bytes, const ZTileIO &io) {
+  if (threadIdx.x == 0) {
+    const uint32_t b = (uint32_t)((bytes + 15) & ~size_t(15));
+    mbar_expect_tx(io.mbar, b);
+    bulk_load(dst, src, b, io.mbar);
+  }
+  const bool ok = mbar_wait_bounded(io.mbar, io.parity);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(io.status, kDevTmaTimeout);
+      mbar_wait_bounded(io.mbar, io.parity);
+    }
+    return false;
+  }
+  return true;
+}
+
+// Outbound bulk copy of the staged bytes; a tail that is not a multiple of 16
+// bytes is stored by thread 0 itself.  Waits until the copy has read shared
+// memory.  The caller has fenced its shared-memory writes and barriered.
+template <typename E>
+__device__ __forceinline__ void bulk_out(E *dst, const E *src, size_t count) {
+  if (threadIdx.x == 0) {
+    const size_t bytes = count * sizeof(E);
+    const size_t body = bytes & ~size_t(15);
+    if (body) {
+      bulk_store(dst, src, (uint32_t)body);
+      bulk_commit();
+    }
+    for (size_t q = body / sizeof(E); q < count; q++) dst[q] = src[q];
+    if (body) bulk_wait_read();
+  }
+}
+
+// R2C along z (ParisPencil.cpp:152-165): the last stage writes Z in natural
+// order into B; the split A[k] = (Z[k] + conj Z[n-k]) / 2,
+// B[k] = (Z[k] - conj Z[n-k]) / (2i) goes out with consecutive threads on
+// consecutive k.
+template <typename T, int N, bool TMAIO, bool TMA_OUT = TMAIO>
+__device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cplx<T>::type *spec, const PassArgs<T> &a,
+                                           int W, int P, long line0, long lend, typename Cplx<T>::type *sm,
+                                           const ZTileIO &io) {
+  using C = typename Cplx<T>::type;
+  const int nk = N > 0 ? N : a.nk;
+  const int nh = a.nh;
+  const int Asz = max(W * P, 2 * W * a.nhp);
+  C *A = sm;
+  C *B = A + ((Asz * (int)sizeof(C) + 127) & ~127) / (int)sizeof(C);
+  const int nl = (int)min((long)(2 * W), lend - line0);
+  const AxisDev<C> &ax = a.ax[2];
+  LineTile<C> tA{A, P}, tB{B, P};
+  LineTileRev<C, typename RevLastOf<N>::type> tBrev{tB, rev_last<N>(ax)};
+  if constexpr (TMAIO) {
+    T *raw = reinterpret_cast<T *>(B);
+    if (!bulk_in(raw, f + line0 * nk, (size_t)nl * nk * sizeof(T), io)) return false;
+    auto ld0 = [&](int pos, int c) -> C {
+      const int la = 2 * c;
+      return mk(la < nl ? raw[la * nk + pos] : (T)0, la + 1 < nl ? raw[(la + 1) * nk + pos] : (T)0);
+    };
+    dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ld0, tA, tBrev, W);
+    // split into the staging rows [line][kh] (pitch nhp) in A, then one copy out
+    const T h = (T)0.5;
+    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+      const int k = it % nh;
+      const int c = it / nh;
+      const C z = tB(k, c);
+      const C w = tB(k == 0 ? 0 : nk - k, c);
+      A[(2 * c) * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
+      A[(2 * c + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    bulk_out(spec + line0 * a.nhp, A, (size_t)nl * a.nhp);
+    return true;
+  } else {
+    auto ldg = [&](int pos, int c) -> C {
+      const long la = line0 + 2 * c;
+      T x = 0, y = 0;
+      if (la < lend) x = f[la * nk + pos];
+      if (la + 1 < lend) y = f[(la + 1) * nk + pos];
+      return mk(x, y);
+    };
+    dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ldg, tA, tBrev, W);
+    const T h = (T)0.5;
+    if constexpr (TMA_OUT) {
+      // staged rows [line][kh] (pitch nhp) in A, then one copy out
+      for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+        const int k = it % nh;
+        const int c = it / nh;
+        const C z = tB(k, c);
+        const C w = tB(k == 0 ? 0 : nk - k, c);
+        A[(2 * c) * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
+        A[(2 * c + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+      }
+      fence_proxy_async_smem();
+      __syncthreads();
+      bulk_out(spec + line0 * a.nhp, A, (size_t)nl * a.nhp);
+    } else {
+      for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+        const int k = it % nh;
+        const int c = it / nh;
+        const long la = line0 + 2 * c;
+        if (la >= lend) continue;
+        const C z = tB(k, c);
+        const C w = tB(k == 0 ? 0 : nk - k, c);
+        spec[la * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
+        if (la + 1 < lend) spec[(la + 1) * a.nhp + k] = mk(h * (z.y + w.y), h * (w.x - z.x));
+      }
+    }
+    return true;
+  }
+}
+
+// C2R along z (ParisPencil.cpp:368-380): Z[k] = A[k] + i B[k] over the
+// Hermitian extension in natural order in B (the imaginary parts of the zero
+// and Nyquist terms are dropped, as a C2R transform does), inverse DIF into
+// natural order in B, real and imaginary parts out to the two lines.
+template <typename T, int N, bool TMAIO>
+__device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T *__restrict__ out,
+                                           const PassArgs<T> &a, int W, int P, long line0, long lend,
+                                           typename Cplx<T>::type *sm, const ZTileIO &io) {
+  using C = typename Cplx<T>::type;
+  const int nk = N > 0 ? N : a.nk;
+  const int nh = a.nh;
+  const int Asz = max(W * P, 2 * W * a.nhp);
+  C *A = sm;
+  C *B = A + ((Asz * (int)sizeof(C) + 127) & ~127) / (int)sizeof(C);
+  const int nl = (int)min((long)(2 * W), lend - line0);
+  const AxisDev<C> &ax = a.ax[2];
+  LineTile<C> tA{A, P}, tB{B, P};
+  LineTileRev<C, typename RevLastOf<N>::type> tBrev{tB, rev_last<N>(ax)};
+  auto hermitian = [&](int k, int c, C sa, C sb) {
+    if (k == 0 || 2 * k == nk) {
+      tB(k, c, mk(sa.x, sb.x));
+    } else {
+      tB(k, c, mk(sa.x - sb.y, sa.y + sb.x));
+      tB(nk - k, c, mk(sa.x + sb.y, sb.x - sa.y));
+    }
+  };
+  if constexpr (TMAIO) {
+    if (!bulk_in(A, spec + line0 * a.nhp, (size_t)nl * a.nhp * sizeof(C), io)) return false;
+    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+      const int k = it % nh;
+      const int c = it / nh;
+      const int la = 2 * c;
+      const C sa = la < nl ? A[la * a.nhp + k] : mk((T)0, (T)0);
+      const C sb = la + 1 < nl ? A[(la + 1) * a.nhp + k] : mk((T)0, (T)0);
+      hermitian(k, c, sa, sb);
+    }
+    __syncthreads();
+    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, tB, tA, tBrev, W);
+    // real lines staged in A, then one copy out
+    T *raw = reinterpret_cast<T *>(A);
+    for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
+      const int t = it % nk;
+      const int c = it / nk;
+      const C v = tB(t, c);
+      raw[(2 * c) * nk + t] = v.x;
+      raw[(2 * c + 1) * nk + t] = v.y;
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    bulk_out(out + line0 * nk, raw, (size_t)nl * nk);
+    return true;
+  } else {
+    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
+      const int k = it % nh;
+      const int c = it / nh;
+      const long la = line0 + 2 * c;
+      C sa = mk((T)0, (T)0), sb = mk((T)0, (T)0);
+      if (la < lend) sa = __ldcg(spec + la * a.nhp + k);
+      if (la + 1 < lend) sb = __ldcg(spec + (la + 1) * a.nhp + k);
+      hermitian(k, c, sa, sb);
+    }
+    __syncthreads();
+    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, tB, tA, tBrev, W);
+    for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
+      const int t = it % nk;
+      const int c = it / nk;
+      const long la = line0 + 2 * c;
+      const C v = tB(t, c);
+      if (la < lend) out[la * nk + t] = v.x;
+      if (la + 1 < lend) out[(la + 1) * nk + t] = v.y;
+    }
+    return true;
+  }
+}
+
+// The last DIF stage of the x forward transform, the filter and the first
+// DIT stage of the inverse act on the same register group.
+template <int R, int W, int NT, int NC, typename C, typename LD, typename ST, typename FL>
+__device__ __forceinline__ void fused_filter_stage(int n_rt, LD &ld, ST &st, FL &filt) {
+  const int n = NC ? NC : n_rt;
+  auto body = [&](int it) {
+    const int c = it % W;
+    const int base = (it / W) * R;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = ld(base + r, c);
+    Dft<R, false, C>::run(v);
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = filt(base + r, c, v[r]);
+    Dft<R, true, C>::run(v);
+#pragma unroll
+    for (int r = 0; r < R; r++) st(base + r, c, v[r]);
+  };
+  if constexpr (NC > 0 && (W * (NC / R)) % NT == 0) {
+    constexpr int ITER = W * (NC / R) / NT;
+#pragma unroll
+    for (int q = 0; q < ITER; q++) body((int)threadIdx.x + q * NT);
+  } else {
+    for (int it = threadIdx.x; it < W * (n / R); it += NT) body(it);
+  }
+}
+
+// 1/x for x > 0 by two Newton-Raphson steps y <- y + y*(1 - x*y) from the
+// single-precision reciprocal (about 2^-23 -> 2^-46 -> full double).
+__device__ __forceinline__ double recip_pos(double x) {
+  double y = (double)__frcp_rn((float)x);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+__device__ __forceinline__ unsigned char *align128(unsigned char *p) {
+  return reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+}
+
+// Twiddle table tw[q] = exp(-2*pi*i*q/n), q < n, from FP64 sincospi.
+template <typename C>
+__global__ void k_twiddles(int n, C *tw) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(2.0 * (double)q / (double)n, &s, &c);   // exp(-2*pi*i*q/n) in FP64
+    tw[q] = mk((decltype(tw[q].x))c, (decltype(tw[q].x))(-s));
+  }
+}
+
+}  // namespace ff

@@ -106,6 +106,47 @@ int ff_plan_check(const ff_plan *plan, void *stream);
 
 int ff_plan_destroy(ff_plan *plan);
 
+/* ---- Batched form (no counterpart in the reference, which solves one grid
+ * per ParisPencil).  `count` independent grids, dims[3g..3g+2] = (ni, nj, nk)
+ * of grid g, each axis 2^a 3^b 5^c and at most 574 points; lo/hi (3 per grid)
+ * give the physical bounds as ParisPencil's constructor takes them
+ * (ParisPencil.hpp:23), or NULL for the reference's domain [-pi, pi - 2pi/n].
+ * A solve of the batch runs the same five passes as ff_solve, each pass one
+ * persistent kernel launch over the tiles of all grids, the five launches
+ * captured once into a CUDA graph and replayed. */
+typedef struct ff_batch ff_batch;
+
+int ff_batch_create(int count, const int *dims, const double *lo, const double *hi, int precision, ff_batch **batch);
+
+/* Bytes each of grid `index`'s two buffers must hold (as ff_plan_bytes). */
+int ff_batch_bytes(const ff_batch *batch, int index, size_t *bytes);
+
+/* Solves every grid: density[g] and potential[g] are device buffers of at
+ * least ff_batch_bytes(g) bytes, 16-byte aligned; density is destroyed.
+ * Asynchronous on `stream` unless `times` is non-NULL (then times->ms[0..4]
+ * are the five passes over all grids).  The first solve, and any solve whose
+ * buffer pointers differ from the previous one, uploads the grid descriptors
+ * and waits for `stream`; solves of one batch must not overlap each other. */
+int ff_batch_solve(ff_batch *batch, void *const *density, void *const *potential, void *stream,
+                   ff_phase_times *times);
+
+/* Autotuner: times each pass with every candidate tile shape for each axis
+ * length of the batch (z passes: line pairs per tile; strided passes:
+ * columns per tile; compile-time or runtime radix plan) and keeps the fastest.
+ * Results are also remembered for batches created later in this process.
+ * The buffers are overwritten (zeroed, then used as scratch); initialise the
+ * densities after tuning.  reps: timed launches per candidate (median). */
+int ff_batch_tune(ff_batch *batch, void *const *density, void *const *potential, void *stream, int reps);
+
+/* The tile shape pass `kind` (0..4) of grid `index` uses: W (line pairs for
+ * the z passes, columns for the strided ones) and ct (1: compile-time plan). */
+int ff_batch_shape(const ff_batch *batch, int index, int kind, int *W, int *ct);
+
+/* As ff_plan_check, for the batch's device status word. */
+int ff_batch_check(ff_batch *batch, void *stream);
+
+int ff_batch_destroy(ff_batch *batch);
+
 /* Harness: write f on the device at x = xlo + i*dx (FishFry.hpp:22-44),
  * plus sum_m a_m cos(k_m.x + theta_m) for the given modes (nmodes may be 0).
  * precision selects a double or float field.  Enqueued on stream. */

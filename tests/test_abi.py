@@ -91,3 +91,18 @@ def test_driver_arguments_checked_on_host(ff):
     assert r.returncode == ff.FF_ERR_TASKS
     r = subprocess.run([exe, "1", "1", "1", "8", "0", "8"], capture_output=True, text=True)
     assert r.returncode == 1
+
+
+@pytest.mark.parametrize("dims,status", [([], "FF_ERR_INVALID"), ([(8, 8, 7)], "FF_ERR_UNSUPPORTED"),
+                                         ([(8, 8, 8), (0, 4, 4)], "FF_ERR_INVALID"),
+                                         ([(576, 8, 8)], "FF_ERR_UNSUPPORTED"), ([(8, 11, 8)], "FF_ERR_UNSUPPORTED")])
+def test_batch_rejects_bad_dims_before_any_device_call(ff, dims, status):
+    with pytest.raises(ff.FFError) as e:
+        ff.Batch(dims)
+    assert e.value.status == getattr(ff, status)
+
+
+def test_batch_rejects_bad_precision(ff):
+    with pytest.raises(ff.FFError) as e:
+        ff.Batch([(8, 8, 8)], precision=5)
+    assert e.value.status == ff.FF_ERR_INVALID

@@ -1,0 +1,143 @@
+"""GPU tests of the batched form (ff_batch_*) against the CPU oracle and the
+single-grid solve.
+
+FP64 bar: each grid's phi within 1e-12 relative L2 of the oracle on the same f.
+FP32 bar: within 1e-5 relative L2 of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+FP32_TOL = 1e-5
+
+# compile-time lengths (32, 48, 64, 80, 96, 128, 256, 512), runtime-plan
+# lengths (27, 30, 36, 45, 50, 60, 75, 100, 120) and one-point / tiny axes
+MIXED = [(32, 48, 64), (80, 96, 128), (36, 45, 50), (64, 64, 64), (128, 32, 96), (27, 30, 25), (1, 8, 6),
+         (60, 1, 100), (120, 75, 2), (16, 16, 16), (256, 8, 12), (6, 512, 4), (10, 12, 512)]
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def make_buffers(torch, batch, precision):
+    dt = torch.float64 if precision == 0 else torch.float32
+    esz = 8 if precision == 0 else 4
+    d = [torch.empty(nb // esz, dtype=dt, device="cuda") for nb in batch.nbytes]
+    p = [torch.empty(nb // esz, dtype=dt, device="cuda") for nb in batch.nbytes]
+    return d, p
+
+
+def init_all(ff, batch, d, modes_of, precision):
+    fs = []
+    for g, n in enumerate(batch.dims):
+        ff.init_field(n, d[g], modes_of(n), precision)
+        N = n[0] * n[1] * n[2]
+        fs.append(d[g][:N].double().cpu().numpy().reshape(n))
+    return fs
+
+
+def results(batch, p):
+    out = []
+    for g, n in enumerate(batch.dims):
+        N = n[0] * n[1] * n[2]
+        out.append(p[g][:N].double().cpu().numpy().reshape(n))
+    return out
+
+
+def modes_for(ff, seed=12345):
+    return lambda n: ff.modes_generate(seed, 64, 32, ff.alias_free_kaxis(n))
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, FP32_TOL)])
+def test_batch_parity_with_oracle(torch_cuda, ff, oracle, precision, tol):
+    batch = ff.Batch(MIXED, precision=precision)
+    d, p = make_buffers(torch_cuda, batch, precision)
+    fs = init_all(ff, batch, d, modes_for(ff), precision)
+    batch.solve(d, p)
+    torch_cuda.cuda.synchronize()
+    batch.check()
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        # the FP64 oracle solves the same (FP32-rounded, for FP32) f
+        assert rel_l2(phi, oracle.solve(f)) <= tol, (g, batch.dims[g])
+
+
+def test_batch_matches_single_grid_solve(torch_cuda, ff):
+    batch = ff.Batch(MIXED)
+    d, p = make_buffers(torch_cuda, batch, 0)
+    init_all(ff, batch, d, modes_for(ff, 7), 0)
+    batch.solve(d, p)
+    got = results(batch, p)
+    for g, n in enumerate(batch.dims):
+        plan = ff.Plan(n)
+        dd = torch_cuda.empty(plan.nbytes // 8, dtype=torch_cuda.float64, device="cuda")
+        pp = torch_cuda.empty_like(dd)
+        ff.init_field(n, dd, modes_for(ff, 7)(n), 0)
+        plan.solve(dd, pp)
+        N = n[0] * n[1] * n[2]
+        ref = pp[:N].cpu().numpy().reshape(n)
+        assert rel_l2(got[g], ref) <= 1e-14, (g, n)
+
+
+def test_batch_graph_replay_is_repeatable(torch_cuda, ff):
+    batch = ff.Batch(MIXED[:6])
+    d, p = make_buffers(torch_cuda, batch, 0)
+    runs = []
+    for _ in range(3):
+        init_all(ff, batch, d, modes_for(ff, 3), 0)
+        ms, tot = batch.solve(d, p, timed=True)
+        assert len(ms) == 5 and tot > 0 and all(x >= 0 for x in ms)
+        runs.append(results(batch, p))
+    for r in runs[1:]:
+        for a, b in zip(runs[0], r):
+            assert np.array_equal(a, b)
+
+
+def test_batch_new_buffers_between_solves(torch_cuda, ff, oracle):
+    batch = ff.Batch(MIXED[:5])
+    for seed in (1, 2):
+        d, p = make_buffers(torch_cuda, batch, 0)
+        fs = init_all(ff, batch, d, modes_for(ff, seed), 0)
+        batch.solve(d, p)
+        for f, phi in zip(fs, results(batch, p)):
+            assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, FP32_TOL)])
+def test_batch_tuned_shapes_keep_parity(torch_cuda, ff, oracle, precision, tol):
+    batch = ff.Batch(MIXED, precision=precision)
+    d, p = make_buffers(torch_cuda, batch, precision)
+    batch.tune(d, p, reps=1)
+    csz = 16 if precision == 0 else 8
+    for g in range(len(batch)):
+        for kind in range(5):
+            W, ct = batch.shape(g, kind)
+            assert W >= 1 and ct in (0, 1)
+            if kind in (1, 2, 3):
+                assert (W * csz) % 128 == 0
+    fs = init_all(ff, batch, d, modes_for(ff), precision)
+    batch.solve(d, p)
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        assert rel_l2(phi, oracle.solve(f)) <= tol, (g, batch.dims[g])
+
+
+def test_batch_of_256_seeded_grids(torch_cuda, ff, oracle):
+    """The batched workload's shape: 256 grids, dims iid from
+    {32, 48, 64, 80, 96, 128}; a sample of grids checked against the oracle,
+    every grid against the analytic potential of its modes."""
+    rng = np.random.default_rng(2024)
+    choices = [32, 48, 64, 80, 96, 128]
+    dims = [tuple(int(x) for x in rng.choice(choices, 3)) for _ in range(256)]
+    batch = ff.Batch(dims)
+    d, p = make_buffers(torch_cuda, batch, 0)
+    fs = init_all(ff, batch, d, modes_for(ff, 99), 0)
+    batch.solve(d, p)
+    torch_cuda.cuda.synchronize()
+    got = results(batch, p)
+    for g in range(0, 256, 37):
+        assert rel_l2(got[g], oracle.solve(fs[g])) <= FP64_TOL, (g, dims[g])
+    for g in range(256):
+        norms = ff.rel_norms(dims[g], p[g], modes_for(ff, 99)(dims[g]), 0)
+        assert max(norms) < 1e-6, (g, dims[g], norms)
