@@ -54,6 +54,14 @@ def parse():
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["solve", "precision", "batch", "serve"], default="solve",
+                    help="solve: one grid (default); precision: 1024^3 FP32 with random modes; "
+                         "batch: 256 seeded grids; serve: Poisson request stream")
+    ap.add_argument("--requests", type=int, default=10000, help="serve: requests per arrival rate")
+    ap.add_argument("--rates", type=float, nargs="+", default=[100, 200, 500, 1000, 2000, 5000],
+                    help="serve: arrival rates (requests/s)")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM admission budget")
+    ap.add_argument("--seed", type=int, default=12345)
     return ap.parse_args()
 
 
@@ -362,10 +370,301 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def modes_for(ff, n, seed, count=64, kmax=32, sigma=0.1):
+    """The seeded random-mode term: count modes, integer 0 < |k| <= kmax,
+    alias-free on grid n, amplitudes N(0, sigma), phases U[0, 2 pi)."""
+    return ff.modes_generate(seed, count, kmax, ff.alias_free_kaxis(n), sigma)
+
+
+def rel_l2_dev(torch, a, b):
+    a = a.double()
+    b = b.double()
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+def run_precision(args):
+    """1024^3 FP32 solve of analytic f + 64 seeded modes; error against the
+    FP64 solve of the same input and against the analytic potential."""
+    import torch
+
+    import fishfry_b200 as ff
+    n = tuple(args.grid) if args.grid != [512, 512, 512] else (1024, 1024, 1024)
+    N = n[0] * n[1] * n[2]
+    modes = modes_for(ff, n, args.seed)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    res = {}
+    for prec in (ff.FF_FP64, ff.FF_FP32):
+        dt = torch.float64 if prec == ff.FF_FP64 else torch.float32
+        plan = ff.Plan(n, precision=prec)
+        esz = 8 if prec == ff.FF_FP64 else 4
+        d = torch.empty(plan.nbytes // esz, dtype=dt, device=dev)
+        p = torch.empty_like(d)
+        f0 = torch.empty(N, dtype=dt, device=dev)
+        ff.init_field(n, f0, modes, prec)
+        times = []
+        for it in range(max(args.warmup, 3) + args.steps):
+            d[:N].copy_(f0)
+            torch.cuda.synchronize()
+            ms, tot = plan.solve(d, p, stream=stream, timed=True)
+            if it >= max(args.warmup, 3):
+                times.append(tot)
+        res[prec] = {"ms": sum(times) / len(times), "phi": p[:N].clone(),
+                     "norms": ff.rel_norms(n, p, modes, prec)}
+        plan.close()
+        del d, p, f0
+        torch.cuda.empty_cache()
+    p64, p32 = res[ff.FF_FP64]["phi"], res[ff.FF_FP32]["phi"]
+    diff = (p32.double() - p64)
+    line = {
+        "metric": "1024^3 FP32 solve points/s (precision form)", "value": N / (res[ff.FF_FP32]["ms"] * 1e-3),
+        "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": res[ff.FF_FP32]["ms"], "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic: analytic f (FishFry.hpp:22-44) + 64 seeded modes, |k| <= 32, a ~ N(0, 0.1)",
+        "config": {"workload": "%dx%dx%d FP32 (FP64 twiddles and 1/k^2)" % n, "modes_seed": args.seed},
+        "fp64_ms_per_solve": res[ff.FF_FP64]["ms"],
+        "fp32_vs_fp64_solve": {"rel_l2": rel_l2_dev(torch, p32, p64),
+                               "rel_linf": float(diff.abs().max() / p64.abs().max())},
+        "fp32_vs_analytic_rel_l1_l2_linf": res[ff.FF_FP32]["norms"],
+        "fp64_vs_analytic_rel_l1_l2_linf": res[ff.FF_FP64]["norms"],
+    }
+    print(json.dumps(line), flush=True)
+
+
+def batch_dims(seed=2024, count=256, choices=(32, 48, 64, 80, 96, 128)):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [tuple(int(x) for x in rng.choice(choices, 3)) for _ in range(count)]
+
+
+def run_batch(args):
+    """256 grids with dims iid from {32, 48, 64, 80, 96, 128}: batched solves
+    (five persistent launches, graph replay, tuned tiles) in FP64 and FP32
+    against a loop of single-grid FP64 solves of the same grids."""
+    import torch
+
+    import fishfry_b200 as ff
+    dims = batch_dims()
+    pts = sum(a * b * c for a, b, c in dims)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    K, W = args.steps, max(args.warmup, 3)
+    out = {}
+    pristine = {}
+    for prec in (ff.FF_FP64, ff.FF_FP32):
+        dt = torch.float64 if prec == ff.FF_FP64 else torch.float32
+        esz = 8 if prec == ff.FF_FP64 else 4
+        b = ff.Batch(dims, precision=prec)
+        d = [torch.empty(nb // esz, dtype=dt, device=dev) for nb in b.nbytes]
+        p = [torch.empty(nb // esz, dtype=dt, device=dev) for nb in b.nbytes]
+        b.tune(d, p, stream=stream, reps=3)
+        f0 = []
+        for g, n in enumerate(dims):
+            x = torch.empty(n[0] * n[1] * n[2], dtype=dt, device=dev)
+            ff.init_field(n, x, modes_for(ff, n, args.seed + g), prec)
+            f0.append(x)
+        pristine[prec] = f0
+
+        def restore():
+            with torch.cuda.stream(stream):
+                for g in range(len(dims)):
+                    d[g][:f0[g].numel()].copy_(f0[g])
+
+        tot = []
+        for it in range(W + K):
+            restore()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.solve(d, p, stream=stream)
+            e1.record(stream)
+            e1.synchronize()
+            if it >= W:
+                tot.append(e0.elapsed_time(e1))
+        ms = sorted(tot)[len(tot) // 2]
+        out[prec] = {"ms": ms, "solves_per_s": len(dims) / (ms * 1e-3), "points_per_s": pts / (ms * 1e-3),
+                     "phi": [x[:f.numel()].clone() for x, f in zip(p, f0)],
+                     "shapes": {k: b.shape(0, k) for k in range(5)}}
+        b.close()
+        del d, p
+        torch.cuda.empty_cache()
+    # loop of single-grid FP64 solves (the plain method, one plan per grid)
+    plans = [ff.Plan(n) for n in dims]
+    ds = [torch.empty(pl.nbytes // 8, dtype=torch.float64, device=dev) for pl in plans]
+    ps = [torch.empty_like(x) for x in ds]
+    tot = []
+    for it in range(W + K):
+        with torch.cuda.stream(stream):
+            for g in range(len(dims)):
+                ds[g][:pristine[ff.FF_FP64][g].numel()].copy_(pristine[ff.FF_FP64][g])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for pl, x, y in zip(plans, ds, ps):
+            pl.solve(x, y, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        if it >= W:
+            tot.append(e0.elapsed_time(e1))
+    loop_ms = sorted(tot)[len(tot) // 2]
+    # accuracy: FP32 batch vs the plain FP64 solve; FP64 batch vs plain FP64
+    err32 = max(rel_l2_dev(torch, a, y[:a.numel()]) for a, y in zip(out[ff.FF_FP32]["phi"], ps))
+    err64 = max(rel_l2_dev(torch, a, y[:a.numel()]) for a, y in zip(out[ff.FF_FP64]["phi"], ps))
+    loop = {"ms": loop_ms, "solves_per_s": len(dims) / (loop_ms * 1e-3)}
+    line = {
+        "metric": "FP32 batched solves/s (256 grids, dims iid {32..128})",
+        "value": out[ff.FF_FP32]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": out[ff.FF_FP32]["ms"], "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic: analytic f + 64 seeded modes per grid", "config": {
+            "workload": "256 grids, dims seed 2024, five persistent launches per solve (CUDA graph), tuned tiles",
+            "points_per_batch": pts},
+        "fp32_batch": {k: v for k, v in out[ff.FF_FP32].items() if k != "phi"},
+        "fp64_batch": {k: v for k, v in out[ff.FF_FP64].items() if k != "phi"},
+        "fp64_loop_of_plain_solves": loop,
+        "fp32_batch_vs_fp64_loop": out[ff.FF_FP32]["solves_per_s"] / loop["solves_per_s"],
+        "fp64_batch_vs_fp64_loop": out[ff.FF_FP64]["solves_per_s"] / loop["solves_per_s"],
+        "max_rel_l2_vs_plain_fp64": {"fp32_batch": err32, "fp64_batch": err64},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _smooth235(n):
+    for q in (2, 3, 5):
+        while n % q == 0:
+            n //= q
+    return n == 1
+
+
+SMOOTH = [n for n in range(32, 513) if _smooth235(n)]
+
+
+def serve_dims(rng):
+    """A 5-smooth triple in [32, 512]^3 whose point count is log-uniform in
+    [32^3, 512^3]: the nearest product among 16 seeded (a, b) draws."""
+    import math
+    target = math.exp(rng.uniform(math.log(32 ** 3), math.log(512 ** 3)))
+    best = None
+    for _ in range(16):
+        a = SMOOTH[rng.integers(len(SMOOTH))]
+        b = SMOOTH[rng.integers(len(SMOOTH))]
+        c = min(SMOOTH, key=lambda x: abs(math.log(a * b * x / target)))
+        err = abs(math.log(a * b * c / target))
+        if best is None or err < best[0]:
+            best = (err, (int(a), int(b), int(c)))
+    return best[1]
+
+
+def run_serve(args):
+    """Poisson arrival stream of mixed-size FP32/FP64 requests through the
+    request loop; p50/p99 latency and solves/s per arrival rate."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    import fishfry_b200 as ff
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed)
+    # request inputs are read from one device source field per precision (the
+    # solve's work does not depend on the values); the accuracy sample below
+    # uses proper fields
+    src = {ff.FF_FP64: torch.randn(512 ** 3, dtype=torch.float64, device=dev, generator=gen),
+           ff.FF_FP32: torch.randn(512 ** 3, dtype=torch.float32, device=dev, generator=gen)}
+    results = []
+    for rate in args.rates:
+        rng = np.random.default_rng(args.seed + int(rate))
+        reqs = [(serve_dims(rng), int(rng.integers(2))) for _ in range(args.requests)]
+        gaps = rng.exponential(1.0 / rate, args.requests)
+        srv = ff.Server(int(args.budget_gb * 1e9), max_active=4096)
+        # warm-up: every axis length's tables resident in both precisions
+        warm = []
+        for L in SMOOTH:
+            for prec in (ff.FF_FP64, ff.FF_FP32):
+                warm.append(srv.submit((L, 32, 32), src[prec], prec))
+        for rid in warm:
+            srv.wait(rid)
+            srv.release(rid)
+        srv.reset_stats()
+        ids = [None] * len(reqs)
+        ready = threading.Event()
+
+        def producer():
+            t0 = time.perf_counter()
+            t = t0
+            for q, (n, prec) in enumerate(reqs):
+                t += gaps[q]
+                while True:
+                    now = time.perf_counter()
+                    if now >= t:
+                        break
+                    if t - now > 0.002:
+                        time.sleep(t - now - 0.001)
+                ids[q] = srv.submit(n, src[prec], prec)
+                if q == 0:
+                    ready.set()
+
+        th = threading.Thread(target=producer)
+        th.start()
+        ready.wait()
+        for q in range(len(reqs)):
+            while ids[q] is None:
+                time.sleep(0.0002)
+            srv.wait(ids[q])
+            srv.release(ids[q])
+        th.join()
+        st = srv.stats()
+        srv.close()
+        results.append({"rate": rate, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                        "max_ms": st["max_ms"], "solves_per_s": st["solves_per_s"],
+                        "points_per_s": st["points_per_s"], "completed": st["completed"],
+                        "peak_gb": st["peak_bytes"] / 1e9, "steps": st["steps"], "launches": st["launches"],
+                        "max_active": st["max_active"]})
+    # accuracy sample: FP32 requests against the plain FP64 solve of the same f
+    srv = ff.Server(int(min(args.budget_gb, 40) * 1e9), max_active=64)
+    rng = np.random.default_rng(args.seed)
+    worst = 0.0
+    for q in range(8):
+        n = serve_dims(rng)
+        if n[0] * n[1] * n[2] > 256 ** 3:
+            continue
+        N = n[0] * n[1] * n[2]
+        f64 = torch.empty(N, dtype=torch.float64, device=dev)
+        ff.init_field(n, f64, modes_for(ff, n, args.seed + q), ff.FF_FP64)
+        f32 = f64.float()
+        rid = srv.submit(n, f32, ff.FF_FP32)
+        srv.wait(rid)
+        o32 = torch.empty(N, dtype=torch.float32, device=dev)
+        srv.fetch(rid, o32)
+        plan = ff.Plan(n)
+        d = torch.empty(plan.nbytes // 8, dtype=torch.float64, device=dev)
+        p = torch.empty_like(d)
+        d[:N].copy_(f32.double())
+        plan.solve(d, p)
+        worst = max(worst, rel_l2_dev(torch, o32, p[:N]))
+    srv.close()
+    line = {
+        "metric": "served solves/s and p99 latency (Poisson arrivals, dims 32..512, FP32:FP64 1:1)",
+        "value": max(r["solves_per_s"] for r in results), "unit": "solves/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f32+f64",
+        "data": "synthetic: request dims log-uniform in points (5-smooth, 32..512 per axis)",
+        "config": {"workload": "continuous batching request loop", "requests_per_rate": args.requests,
+                   "budget_gb": args.budget_gb, "seed": args.seed},
+        "rates": results,
+        "fp32_vs_plain_fp64_rel_l2_max": worst,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "precision":
+        run_precision(args)
+    elif args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

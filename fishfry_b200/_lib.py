@@ -31,6 +31,8 @@ EXPORTS = [
     "ff_last_error", "ff_version",
     "ff_batch_create", "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
     "ff_batch_destroy",
+    "ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_fetch", "ff_server_release",
+    "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy",
 ]
 
 
@@ -49,6 +51,22 @@ class Mode(ctypes.Structure):
 
 class PhaseTimes(ctypes.Structure):
     _fields_ = [("count", ctypes.c_int), ("ms", ctypes.c_double * FF_MAX_PHASES), ("total_ms", ctypes.c_double)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_active", ctypes.c_int)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("latency_ms", ctypes.c_double), ("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double)]
+
+
+class ServerReport(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("p50_ms", ctypes.c_double),
+                ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("solves_per_s", ctypes.c_double), ("points_per_s", ctypes.c_double),
+                ("peak_bytes", ctypes.c_size_t), ("budget_bytes", ctypes.c_size_t), ("steps", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("max_active", ctypes.c_int)]
 
 
 _lib = None
@@ -85,6 +103,18 @@ def _declare(L):
     L.ff_batch_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
     L.ff_batch_check.argtypes = [vp, vp]
     L.ff_batch_destroy.argtypes = [vp]
+    L.ff_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+    L.ff_server_submit.argtypes = [vp, i3, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]
+    L.ff_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestInfo)]
+    L.ff_server_fetch.argtypes = [vp, ctypes.c_uint64, vp, ctypes.c_int]
+    L.ff_server_release.argtypes = [vp, ctypes.c_uint64]
+    L.ff_server_stats.argtypes = [vp, ctypes.POINTER(ServerReport)]
+    L.ff_server_check.argtypes = [vp]
+    L.ff_server_reset_stats.argtypes = [vp]
+    L.ff_server_destroy.argtypes = [vp]
+    for name in ("ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_fetch", "ff_server_release",
+                 "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy"):
+        getattr(L, name).restype = ctypes.c_int
     for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
                  "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_batch_create",
                  "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",

@@ -165,6 +165,74 @@ class Batch:
             pass
 
 
+class Server:
+    """Request loop with continuous batching (ff_server_*): submit solves of
+    mixed sizes and precisions; each result is ready after `wait`.
+
+    hbm_budget: bytes of device memory for request buffers; max_active:
+    requests on the device at once per precision.
+    """
+
+    def __init__(self, hbm_budget, max_active=1024):
+        cfg = _lib.ServerConfig(int(hbm_budget), int(max_active))
+        h = ctypes.c_void_p()
+        check(lib().ff_server_create(ctypes.byref(cfg), ctypes.byref(h)), "ff_server_create")
+        self._h = h
+        self._inputs = {}
+
+    def submit(self, n, f, precision=FF_FP64, on_host=None):
+        """Queue a solve of field f (torch tensor on the device or pinned host
+        tensor, or an int device address); returns the request id.  f is kept
+        alive until the request is fetched or released."""
+        if on_host is None:
+            on_host = not isinstance(f, int) and not f.is_cuda
+        rid = ctypes.c_uint64()
+        check(lib().ff_server_submit(self._h, int3(n), int(precision), _ptr(f), int(bool(on_host)), ctypes.byref(rid)),
+              "ff_server_submit")
+        self._inputs[rid.value] = f
+        return rid.value
+
+    def wait(self, rid, timeout_ms=-1.0):
+        """Blocks until request rid is done; returns (latency, queue, run) ms."""
+        info = _lib.RequestInfo()
+        check(lib().ff_server_wait(self._h, int(rid), float(timeout_ms), ctypes.byref(info)), "ff_server_wait")
+        return info.latency_ms, info.queue_ms, info.run_ms
+
+    def fetch(self, rid, out=None, on_host=None):
+        """Copies the potential into `out` (device or host tensor; None: drop) and releases the request."""
+        if on_host is None:
+            on_host = out is not None and not isinstance(out, int) and not out.is_cuda
+        check(lib().ff_server_fetch(self._h, int(rid), _ptr(out), int(bool(on_host))), "ff_server_fetch")
+        self._inputs.pop(rid, None)
+
+    def release(self, rid):
+        check(lib().ff_server_release(self._h, int(rid)), "ff_server_release")
+        self._inputs.pop(rid, None)
+
+    def stats(self):
+        r = _lib.ServerReport()
+        check(lib().ff_server_stats(self._h, ctypes.byref(r)), "ff_server_stats")
+        return {k: getattr(r, k) for k, _ in r._fields_}
+
+    def reset_stats(self):
+        check(lib().ff_server_reset_stats(self._h), "ff_server_reset_stats")
+
+    def check(self):
+        check(lib().ff_server_check(self._h), "ff_server_check")
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            check(lib().ff_server_destroy(self._h), "ff_server_destroy")
+            self._h = ctypes.c_void_p()
+            self._inputs.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class ParisPencil:
     """The reference plugin interface (ParisPencil.hpp:11-59) on one GPU.
 

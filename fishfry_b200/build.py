@@ -18,9 +18,9 @@ LIB = os.path.join(HERE, "lib", "libfishfry.so")
 BIN = os.path.join(HERE, "bin", "fishfry")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUDE]
+NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-pthread", "-I" + INCLUDE]
 
-LIB_SOURCES = ["ff_solve.cu", "ff_field.cu", "ff_batch.cu", "ff_batch_f64.cu", "ff_batch_f32.cu"]
+LIB_SOURCES = ["ff_solve.cu", "ff_field.cu", "ff_batch.cu", "ff_batch_f64.cu", "ff_batch_f32.cu", "ff_serve.cu"]
 HEADERS = ["ff_fft.cuh", "ff_tiles.cuh", "ff_status.hpp", "ff_batch.hpp", "ff_batch_dev.cuh"]
 
 
@@ -60,7 +60,7 @@ def build_lib(verbose=False, force=False):
         for f in [ex.submit(_run, [_nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o], verbose) for s, o in zip(srcs, objs)]:
             f.result()
     tmp = LIB + ".tmp"
-    _run([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"], verbose)
+    _run([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-lpthread"], verbose)
     os.replace(tmp, LIB)
     for o in objs:
         os.remove(o)

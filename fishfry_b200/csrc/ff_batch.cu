@@ -29,11 +29,6 @@ std::vector<int> plan_digit_reversal(int n, const std::vector<int> &radix);
 
 namespace {
 
-struct AxisSlot {
-  int n;
-  size_t o_tw, o_tw64, o_rev, o_ipos;
-};
-
 // Tuned shapes, process-wide: (precision, pass kind, axis length) -> shape.
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int>, TileShape> g_tuned;
@@ -55,7 +50,6 @@ struct ff_batch {
   std::vector<size_t> bytes;
   void *dmem = nullptr;          // axis tables, status, tickets, descriptors, work lists
   size_t dmem_size = 0;
-  std::vector<AxisSlot> axes;
   int *status = nullptr;
   int *tickets = nullptr;        // one per pass
   void *desc = nullptr;          // device grid descriptors
@@ -96,10 +90,11 @@ int pass_launch(const ff_batch *b, int kind, cudaStream_t st) {
                                  : batch_pass_launch<float>(kind, b->desc, wl, b->blocks[kind], b->smem[kind], st);
 }
 
-int axis_len(const BatchGridHost &g, int kind) { return g.n[axis_of_kind(kind)]; }
+}  // namespace
 
-// Tiles of one pass of one grid.
-int tiles_of(const BatchGridHost &g, int kind) {
+int batch_axis_len(const BatchGridHost &g, int kind) { return g.n[axis_of_kind(kind)]; }
+
+int batch_tiles_of(const BatchGridHost &g, int kind) {
   const TileShape &s = g.shape[kind];
   if (kind == 0 || kind == 4) {
     const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
@@ -109,38 +104,39 @@ int tiles_of(const BatchGridHost &g, int kind) {
   return (int)((ncols + s.W - 1) / s.W);
 }
 
-size_t shape_smem(const ff_batch *b, const BatchGridHost &g, int kind, const TileShape &s) {
-  return batch_tile_smem(kind, axis_len(g, kind), g.n[2], g.nhp, s.W, b->csz);
+size_t batch_shape_smem(int precision, const BatchGridHost &g, int kind, const TileShape &s) {
+  return batch_tile_smem(kind, batch_axis_len(g, kind), g.n[2], g.nhp, s.W, precision == FF_FP64 ? 16 : 8);
 }
 
-bool shape_valid(const ff_batch *b, const BatchGridHost &g, int kind, const TileShape &s) {
+bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const TileShape &s) {
   if (s.W < 1) return false;
-  if (s.ct && !batch_special_n(axis_len(g, kind))) return false;
+  if (s.ct && !batch_special_n(batch_axis_len(g, kind))) return false;
   if (kind != 0 && kind != 4) {
-    const int w1 = 128 / (int)b->csz;
+    const int w1 = 128 / (precision == FF_FP64 ? 16 : 8);
     if (s.W != w1 && s.W != 2 * w1 && s.W != 4 * w1) return false;
   }
-  return shape_smem(b, g, kind, s) <= kBatchSmem;
+  return batch_shape_smem(precision, g, kind, s) <= kBatchSmem;
 }
 
-// Default shape: about 256 butterfly items per stage (one per thread) within
-// the shared-memory budget; compile-time tiles where the length has them.
-TileShape default_shape(const ff_batch *b, const BatchGridHost &g, int kind) {
-  const int n = axis_len(g, kind);
+// Default shape: tiles of about 4096 points (256 threads, a few butterfly
+// items each per stage) within the shared-memory budget; compile-time tiles
+// where the length has them.
+TileShape batch_default_shape(int precision, const BatchGridHost &g, int kind) {
+  const int n = batch_axis_len(g, kind);
   TileShape s{1, batch_special_n(n) ? 1 : 0};
   if (kind == 0 || kind == 4) {
     const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
     int W = std::max(1, 2048 / std::max(1, g.n[2]));
     W = (int)std::min<long>(W, npairs);
-    while (W > 1 && !shape_valid(b, g, kind, TileShape{W, s.ct})) W--;
+    while (W > 1 && !batch_shape_valid(precision, g, kind, TileShape{W, s.ct})) W--;
     s.W = W;
     return s;
   }
-  const int w1 = 128 / (int)b->csz;
+  const int w1 = 128 / (precision == FF_FP64 ? 16 : 8);
   int W = w1;
   for (int m = 4; m >= 1; m /= 2) {
     const TileShape t{m * w1, s.ct};
-    if (m * w1 * n <= 2048 * 2 && shape_valid(b, g, kind, t)) {
+    if (m * w1 * n <= 4096 && batch_shape_valid(precision, g, kind, t)) {
       W = m * w1;
       break;
     }
@@ -149,14 +145,91 @@ TileShape default_shape(const ff_batch *b, const BatchGridHost &g, int kind) {
   return s;
 }
 
-TileShape tuned_or_default(const ff_batch *b, const BatchGridHost &g, int kind) {
+TileShape batch_shape_for(int precision, const BatchGridHost &g, int kind) {
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned.find(std::make_tuple(b->precision, kind, axis_len(g, kind)));
-    if (it != g_tuned.end() && shape_valid(b, g, kind, it->second)) return it->second;
+    auto it = g_tuned.find(std::make_tuple(precision, kind, batch_axis_len(g, kind)));
+    if (it != g_tuned.end() && batch_shape_valid(precision, g, kind, it->second)) return it->second;
   }
-  return default_shape(b, g, kind);
+  return batch_default_shape(precision, g, kind);
 }
+
+size_t batch_axis_bytes(int n, int precision) {
+  const size_t csz = precision == FF_FP64 ? 16 : 8;
+  auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return r(n * csz) + (precision == FF_FP64 ? 0 : r(n * sizeof(double2))) + 2 * r(n * sizeof(int));
+}
+
+int batch_axis_build(int n, int precision, void *mem, AxisDev<double2> *ad, AxisDev<float2> *af, cudaStream_t st) {
+  const size_t csz = precision == FF_FP64 ? 16 : 8;
+  auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
+  char *base = static_cast<char *>(mem);
+  const size_t o_tw = 0;
+  const size_t o_tw64 = precision == FF_FP64 ? o_tw : r(n * csz);
+  const size_t o_rev = precision == FF_FP64 ? r(n * csz) : o_tw64 + r(n * sizeof(double2));
+  const size_t o_ipos = o_rev + r(n * sizeof(int));
+  const std::vector<int> radix = plan_factor_radices(n);
+  const std::vector<int> rev = plan_digit_reversal(n, radix);
+  std::vector<int> ipos(n);
+  for (int q = 0; q < n; q++) ipos[rev[q]] = q;
+  FF_CUDA(cudaMemcpyAsync(base + o_rev, rev.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+  FF_CUDA(cudaMemcpyAsync(base + o_ipos, ipos.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+  const int blocks = std::min(1024, (n + 255) / 256);
+  k_twiddles<<<blocks, 256, 0, st>>>(n, reinterpret_cast<double2 *>(base + o_tw64));
+  if (precision == FF_FP32) k_twiddles<<<blocks, 256, 0, st>>>(n, reinterpret_cast<float2 *>(base + o_tw));
+  FF_CUDA(cudaGetLastError());
+  // the host vectors above must outlive the copies
+  FF_CUDA(cudaStreamSynchronize(st));
+  *ad = AxisDev<double2>{};
+  *af = AxisDev<float2>{};
+  ad->n = af->n = n;
+  ad->nstages = af->nstages = (int)radix.size();
+  for (size_t q = 0; q < radix.size(); q++) ad->radix[q] = af->radix[q] = radix[q];
+  ad->tw = reinterpret_cast<const double2 *>(base + o_tw);
+  af->tw = reinterpret_cast<const float2 *>(base + o_tw);
+  ad->tw64 = af->tw64 = reinterpret_cast<const double2 *>(base + o_tw64);
+  ad->rev = af->rev = reinterpret_cast<const int *>(base + o_rev);
+  ad->ipos = af->ipos = reinterpret_cast<const int *>(base + o_ipos);
+  return FF_OK;
+}
+
+void batch_grid_init(BatchGridHost &h, const int n[3], const double *lo, const double *hi, int precision) {
+  std::memset(&h, 0, sizeof(h));
+  for (int d = 0; d < 3; d++) {
+    h.n[d] = n[d];
+    // ParisPencil.cpp:9-11; the reference domain [-pi, pi - 2pi/n] when no bounds are given
+    const double len = (lo && hi) ? hi[d] - lo[d] : 2.0 * M_PI * double(n[d] - 1) / double(n[d]);
+    h.dd[d] = n[d] > 1 ? 2.0 * M_PI * double(n[d] - 1) / (double(n[d]) * len) : 0.0;
+  }
+  h.nh = h.n[2] / 2 + 1;
+  h.nhp = precision == FF_FP64 ? h.nh : (h.nh + 1) & ~1;
+  h.invN = 1.0 / (double(h.n[0]) * double(h.n[1]) * double(h.n[2]));
+}
+
+size_t batch_grid_bytes(const BatchGridHost &h, int precision) {
+  const size_t csz = precision == FF_FP64 ? 16 : 8;
+  const size_t spec = (size_t)h.n[0] * h.n[1] * h.nhp * csz;
+  const size_t real = (size_t)h.n[0] * h.n[1] * h.n[2] * (csz / 2);
+  return std::max(spec, real);
+}
+
+int batch_check_dims(const int n[3], const double *lo, const double *hi, const char *who, int g) {
+  for (int d = 0; d < 3; d++) {
+    if (n[d] < 1) return set_error(FF_ERR_INVALID, "%s: grid %d n[%d] = %d < 1", who, g, d, n[d]);
+    if (n[d] > FF_MAX_AXIS || !smooth235(n[d]))
+      return set_error(FF_ERR_UNSUPPORTED, "%s: grid %d n[%d] = %d is not 2^a 3^b 5^c <= %d", who, g, d, n[d],
+                       FF_MAX_AXIS);
+    if (lo && hi && n[d] > 1 && !(hi[d] > lo[d]))
+      return set_error(FF_ERR_INVALID, "%s: grid %d hi[%d] <= lo[%d]", who, g, d, d);
+    // the narrowest tile of a strided pass holds whole lines of 128-byte rows
+    if ((size_t)n[d] * 128 + 128 > kBatchSmem)
+      return set_error(FF_ERR_UNSUPPORTED, "%s: grid %d axis of %d points exceeds the batch tiles (%zu)", who, g,
+                       n[d], (kBatchSmem - 128) / 128);
+  }
+  return FF_OK;
+}
+
+namespace {
 
 // Work lists, block counts and shared memory of every pass from the grids'
 // current shapes; uploads lists and descriptors (synchronously).
@@ -167,8 +240,8 @@ int build_work(ff_batch *b) {
     size_t smem = 256;
     for (int g = 0; g < b->count; g++) {
       ent[g] = make_int2(g, k);
-      start[g + 1] = start[g] + tiles_of(b->grids[g], k);
-      smem = std::max(smem, shape_smem(b, b->grids[g], k, b->grids[g].shape[k]));
+      start[g + 1] = start[g] + batch_tiles_of(b->grids[g], k);
+      smem = std::max(smem, batch_shape_smem(b->precision, b->grids[g], k, b->grids[g].shape[k]));
     }
     b->ntiles[k] = start[b->count];
     b->smem[k] = smem;
@@ -290,20 +363,11 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
   if (count < 1 || !dims) return set_error(FF_ERR_INVALID, "ff_batch_create: count %d or dims missing", count);
   if (precision != FF_FP64 && precision != FF_FP32)
     return set_error(FF_ERR_INVALID, "ff_batch_create: precision %d is neither FF_FP64 nor FF_FP32", precision);
-  for (int g = 0; g < count; g++)
-    for (int d = 0; d < 3; d++) {
-      const int n = dims[3 * g + d];
-      if (n < 1) return set_error(FF_ERR_INVALID, "ff_batch_create: grid %d n[%d] = %d < 1", g, d, n);
-      if (n > FF_MAX_AXIS || !smooth235(n))
-        return set_error(FF_ERR_UNSUPPORTED, "ff_batch_create: grid %d n[%d] = %d is not 2^a 3^b 5^c <= %d", g, d,
-                         n, FF_MAX_AXIS);
-      if (lo && hi && n > 1 && !(hi[3 * g + d] > lo[3 * g + d]))
-        return set_error(FF_ERR_INVALID, "ff_batch_create: grid %d hi[%d] <= lo[%d]", g, d, d);
-      // the narrowest tile of a strided pass holds whole lines of 128-byte rows
-      if ((size_t)n * 128 + 128 > kBatchSmem)
-        return set_error(FF_ERR_UNSUPPORTED, "ff_batch_create: grid %d axis of %d points exceeds the batch tiles (%zu)",
-                         g, n, (kBatchSmem - 128) / 128);
-    }
+  for (int g = 0; g < count; g++) {
+    const int rc = batch_check_dims(dims + 3 * g, lo ? lo + 3 * g : nullptr, hi ? hi + 3 * g : nullptr,
+                                    "ff_batch_create", g);
+    if (rc != FF_OK) return rc;
+  }
   ff_batch *b = new ff_batch();
   b->count = count;
   b->precision = precision;
@@ -315,20 +379,13 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
   }
   b->desc_size = desc_size(precision);
   // distinct axis lengths -> one table set each
-  std::map<int, int> slot_of;
+  std::map<int, size_t> table_of;
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
   for (int g = 0; g < count; g++)
     for (int d = 0; d < 3; d++) {
       const int n = dims[3 * g + d];
-      if (slot_of.count(n)) continue;
-      AxisSlot s{n, 0, 0, 0, 0};
-      s.o_tw = take(n * b->csz);
-      s.o_tw64 = precision == FF_FP64 ? s.o_tw : take(n * sizeof(double2));
-      s.o_rev = take(n * sizeof(int));
-      s.o_ipos = take(n * sizeof(int));
-      slot_of[n] = (int)b->axes.size();
-      b->axes.push_back(s);
+      if (!table_of.count(n)) table_of[n] = take(batch_axis_bytes(n, precision));
     }
   const size_t o_status = take(sizeof(int));
   const size_t o_tickets = take(5 * sizeof(int));
@@ -339,7 +396,6 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
     o_start[k] = take((size_t)(count + 1) * sizeof(int));
   }
   b->dmem_size = off;
-  int rc = FF_OK;
   if (cudaMalloc(&b->dmem, off) != cudaSuccess) {
     cudaGetLastError();
     delete b;
@@ -359,63 +415,33 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
     b->entries[k] = reinterpret_cast<int2 *>(base + o_ent[k]);
     b->starts[k] = reinterpret_cast<int *>(base + o_start[k]);
   }
+  int rc = FF_OK;
   if (cudaMemset(b->status, 0, sizeof(int)) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_create: memset");
+  if (rc == FF_OK && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
+    rc = set_error(FF_ERR_CUDA, "ff_batch_create: stream");
   // axis tables: twiddles from FP64 sincospi, digit reversal of the default plan
-  std::vector<AxisDev<double2>> axd(b->axes.size());
-  std::vector<AxisDev<float2>> axf(b->axes.size());
-  for (size_t a = 0; a < b->axes.size() && rc == FF_OK; a++) {
-    const AxisSlot &s = b->axes[a];
-    const std::vector<int> radix = plan_factor_radices(s.n);
-    const std::vector<int> rev = plan_digit_reversal(s.n, radix);
-    std::vector<int> ipos(s.n);
-    for (int q = 0; q < s.n; q++) ipos[rev[q]] = q;
-    if (cudaMemcpy(base + s.o_rev, rev.data(), s.n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(base + s.o_ipos, ipos.data(), s.n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
-      rc = set_error(FF_ERR_CUDA, "ff_batch_create: table upload failed");
-    const int blocks = std::min(1024, (s.n + 255) / 256);
-    k_twiddles<<<blocks, 256>>>(s.n, reinterpret_cast<double2 *>(base + s.o_tw64));
-    if (precision == FF_FP32) k_twiddles<<<blocks, 256>>>(s.n, reinterpret_cast<float2 *>(base + s.o_tw));
-    AxisDev<double2> ad{};
-    AxisDev<float2> af{};
-    ad.n = af.n = s.n;
-    ad.nstages = af.nstages = (int)radix.size();
-    for (size_t q = 0; q < radix.size(); q++) ad.radix[q] = af.radix[q] = radix[q];
-    ad.tw = reinterpret_cast<const double2 *>(base + s.o_tw);
-    af.tw = reinterpret_cast<const float2 *>(base + s.o_tw);
-    ad.tw64 = af.tw64 = reinterpret_cast<const double2 *>(base + s.o_tw64);
-    ad.rev = af.rev = reinterpret_cast<const int *>(base + s.o_rev);
-    ad.ipos = af.ipos = reinterpret_cast<const int *>(base + s.o_ipos);
-    axd[a] = ad;
-    axf[a] = af;
+  std::map<int, std::pair<AxisDev<double2>, AxisDev<float2>>> axes;
+  for (const auto &t : table_of) {
+    if (rc != FF_OK) break;
+    AxisDev<double2> ad;
+    AxisDev<float2> af;
+    rc = batch_axis_build(t.first, precision, base + t.second, &ad, &af, b->cap);
+    axes[t.first] = std::make_pair(ad, af);
   }
-  if (rc == FF_OK && (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess))
-    rc = set_error(FF_ERR_CUDA, "ff_batch_create: table kernels failed");
   b->grids.resize(count);
   b->bytes.resize(count);
   for (int g = 0; g < count && rc == FF_OK; g++) {
     BatchGridHost &h = b->grids[g];
-    std::memset(&h, 0, sizeof(h));
+    batch_grid_init(h, dims + 3 * g, lo ? lo + 3 * g : nullptr, hi ? hi + 3 * g : nullptr, precision);
     for (int d = 0; d < 3; d++) {
-      const int n = dims[3 * g + d];
-      h.n[d] = n;
-      // ParisPencil.cpp:9-11; the reference domain [-pi, pi - 2pi/n] when no bounds are given
-      const double len = (lo && hi) ? hi[3 * g + d] - lo[3 * g + d] : 2.0 * M_PI * double(n - 1) / double(n);
-      h.dd[d] = n > 1 ? 2.0 * M_PI * double(n - 1) / (double(n) * len) : 0.0;
-      h.axd[d] = axd[slot_of[n]];
-      h.axf[d] = axf[slot_of[n]];
+      h.axd[d] = axes[h.n[d]].first;
+      h.axf[d] = axes[h.n[d]].second;
     }
-    h.nh = h.n[2] / 2 + 1;
-    h.nhp = precision == FF_FP64 ? h.nh : (h.nh + 1) & ~1;
-    h.invN = 1.0 / (double(h.n[0]) * double(h.n[1]) * double(h.n[2]));
     h.status = b->status;
-    const size_t spec = (size_t)h.n[0] * h.n[1] * h.nhp * b->csz;
-    const size_t real = (size_t)h.n[0] * h.n[1] * h.n[2] * (b->csz / 2);
-    b->bytes[g] = std::max(spec, real);
-    for (int k = 0; k < 5; k++) h.shape[k] = tuned_or_default(b, h, k);
+    b->bytes[g] = batch_grid_bytes(h, precision);
+    for (int k = 0; k < 5; k++) h.shape[k] = batch_shape_for(precision, h, k);
   }
   if (rc == FF_OK) rc = build_work(b);
-  if (rc == FF_OK && cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
-    rc = set_error(FF_ERR_CUDA, "ff_batch_create: stream");
   for (int e = 0; e < 6 && rc == FF_OK; e++)
     if (cudaEventCreate(&b->ev[e]) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_create: event");
   if (rc != FF_OK) {
@@ -490,16 +516,16 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
   drop_graph(b);
   for (int k = 0; k < 5; k++) {
     std::vector<int> lens;
-    for (const auto &g : b->grids) lens.push_back(axis_len(g, k));
+    for (const auto &g : b->grids) lens.push_back(batch_axis_len(g, k));
     std::sort(lens.begin(), lens.end());
     lens.erase(std::unique(lens.begin(), lens.end()), lens.end());
     for (int n : lens) {
       int first = -1;
       for (int g = 0; g < b->count; g++)
-        if (axis_len(b->grids[g], k) == n) { first = g; break; }
+        if (batch_axis_len(b->grids[g], k) == n) { first = g; break; }
       const BatchGridHost &ref = b->grids[first];
       std::vector<TileShape> cand;
-      const TileShape d = default_shape(b, ref, k);
+      const TileShape d = batch_default_shape(b->precision, ref, k);
       for (int ct = batch_special_n(n) ? 1 : 0; ct >= 0; ct--) {
         if (k == 0 || k == 4) {
           for (int W : {std::max(1, d.W / 2), d.W, d.W * 2}) cand.push_back(TileShape{W, ct});
@@ -513,10 +539,10 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
       for (const TileShape &c : cand) {
         bool ok = true;
         for (const auto &g : b->grids)
-          if (axis_len(g, k) == n && !shape_valid(b, g, k, c)) ok = false;
+          if (batch_axis_len(g, k) == n && !batch_shape_valid(b->precision, g, k, c)) ok = false;
         if (!ok) continue;
         for (auto &g : b->grids)
-          if (axis_len(g, k) == n) g.shape[k] = c;
+          if (batch_axis_len(g, k) == n) g.shape[k] = c;
         rc = build_work(b);
         if (rc == FF_OK) rc = upload_desc(b, st);
         float ms = 0;
@@ -528,7 +554,7 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
         }
       }
       for (auto &g : b->grids)
-        if (axis_len(g, k) == n) g.shape[k] = best;
+        if (batch_axis_len(g, k) == n) g.shape[k] = best;
       std::lock_guard<std::mutex> lk(g_tune_mu);
       g_tuned[std::make_tuple(b->precision, k, n)] = best;
     }

@@ -88,4 +88,21 @@ struct BatchGridHost {
   TileShape shape[5];
 };
 
+// Host helpers shared by the batch and the server (ff_batch.cu).
+int batch_axis_len(const BatchGridHost &g, int kind);
+int batch_tiles_of(const BatchGridHost &g, int kind);
+size_t batch_shape_smem(int precision, const BatchGridHost &g, int kind, const TileShape &s);
+bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const TileShape &s);
+TileShape batch_default_shape(int precision, const BatchGridHost &g, int kind);
+// The tuned shape for (precision, kind, axis length) if the tuner has one, else the default.
+TileShape batch_shape_for(int precision, const BatchGridHost &g, int kind);
+// Device bytes of one axis's tables, and their construction at mem (waits for st).
+size_t batch_axis_bytes(int n, int precision);
+int batch_axis_build(int n, int precision, void *mem, AxisDev<double2> *ad, AxisDev<float2> *af, cudaStream_t st);
+// Dimensions, wavenumber scales (lo/hi: 3 values or NULL), nh/nhp, 1/N.
+void batch_grid_init(BatchGridHost &h, const int n[3], const double *lo, const double *hi, int precision);
+size_t batch_grid_bytes(const BatchGridHost &h, int precision);
+// Axis checks of one grid (status and message as the C ABI reports them).
+int batch_check_dims(const int n[3], const double *lo, const double *hi, const char *who, int g);
+
 }  // namespace ff

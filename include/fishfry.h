@@ -147,6 +147,70 @@ int ff_batch_check(ff_batch *batch, void *stream);
 
 int ff_batch_destroy(ff_batch *batch);
 
+/* ---- Serving form (no counterpart in the reference).  A request loop on a
+ * library thread takes solves of mixed sizes and precisions as they arrive,
+ * admits them against an HBM budget, and runs them with continuous batching:
+ * every scheduling step carries each admitted request one pass further, all
+ * requests at the same pass sharing one persistent launch (the batch
+ * kernels), so requests that arrive while others run join the next step.
+ * Axis tables stay resident per (length, precision); the device memory of
+ * the requests' buffers is one arena of hbm_budget bytes reserved at
+ * creation.  Each request's result is bit-identical whether it runs alone or
+ * in a mix (its tiles and their arithmetic do not depend on the mix). */
+typedef struct ff_server ff_server;
+
+typedef struct {
+  size_t hbm_budget; /* bytes reserved for request buffers (2 x ff_plan_bytes per request) */
+  int max_active;    /* requests admitted at once (descriptor slots per precision) */
+} ff_server_config;
+
+typedef struct {
+  double latency_ms; /* submit -> result ready on the device */
+  double queue_ms;   /* submit -> admitted (buffers reserved, input copy issued) */
+  double run_ms;     /* admitted -> result ready */
+} ff_request_info;
+
+typedef struct {
+  uint64_t submitted, completed;
+  double p50_ms, p99_ms, mean_ms, max_ms; /* latency over completed requests */
+  double solves_per_s, points_per_s;      /* completed over first submit .. last completion */
+  size_t peak_bytes, budget_bytes;        /* arena high-water mark and budget */
+  uint64_t steps, launches;               /* scheduling steps and kernel launches so far */
+  int max_active;                         /* most requests on the device at once */
+} ff_server_report;
+
+int ff_server_create(const ff_server_config *cfg, ff_server **server);
+
+/* Queues a solve of the real field f (ni*nj*nk values of the precision's
+ * type, x slowest) on the reference domain of n.  f is a host pointer
+ * (f_on_host = 1; pinned memory avoids a staged copy) or a device pointer,
+ * and must stay valid until ff_server_wait reports the request done.
+ * FF_ERR_NOMEM if the request alone exceeds the budget. */
+int ff_server_submit(ff_server *server, const int n[3], int precision, const void *f, int f_on_host, uint64_t *id);
+
+/* Waits up to timeout_ms (< 0: without limit) for the request; FF_OK when
+ * its result is ready, FF_ERR_TIMEOUT otherwise.  info may be NULL. */
+int ff_server_wait(ff_server *server, uint64_t id, double timeout_ms, ff_request_info *info);
+
+/* Copies a finished request's potential (ni*nj*nk values) to phi (host or
+ * device; phi NULL copies nothing) and releases the request's buffers. */
+int ff_server_fetch(ff_server *server, uint64_t id, void *phi, int phi_on_host);
+
+/* Releases a finished (or not yet admitted) request without copying. */
+int ff_server_release(ff_server *server, uint64_t id);
+
+int ff_server_stats(ff_server *server, ff_server_report *stats);
+
+/* Clears the latency record and counters (e.g. after a warm-up). */
+int ff_server_reset_stats(ff_server *server);
+
+/* FF_ERR_TIMEOUT if a kernel's bounded wait gave up; the scheduler's error if
+ * it stopped. */
+int ff_server_check(ff_server *server);
+
+/* Stops the loop (requests still queued are dropped) and frees everything. */
+int ff_server_destroy(ff_server *server);
+
 /* Harness: write f on the device at x = xlo + i*dx (FishFry.hpp:22-44),
  * plus sum_m a_m cos(k_m.x + theta_m) for the given modes (nmodes may be 0).
  * precision selects a double or float field.  Enqueued on stream. */
