@@ -38,8 +38,8 @@ L2_BYTES = 126 * 1024 * 1024
 # profiles/passes_fp64_512cube_ncu_full.txt.
 MEASURED_TRAFFIC = {
     ("512x512x512", "fp64"): {
-        "Real-to-complex FFT in Z": 2.104563e9, "Forward FFT in Y": 2.102818e9, "X FFTs and filter": 2.102127e9,
-        "Backward FFT in Y": 2.104016e9, "Complex-to-real FFT in Z": 2.104495e9,
+        "Real-to-complex FFT in Z": 2.105426e9, "Forward FFT in Y": 2.102568e9, "X FFTs and filter": 2.110848e9,
+        "Backward FFT in Y": 2.105730e9, "Complex-to-real FFT in Z": 2.104985e9,
     },
 }
 
@@ -198,13 +198,37 @@ def oracle_baseline(n, threads=None, steps=1, warmup=1):
     return times, cores
 
 
+def reference_sample_grid(n, steps, budget_s=150.0):
+    """The largest cube sample (of the workload's kind, at most n) whose
+    steps + warm-up finish within budget_s on the host cores, from a timed
+    128^3 solve scaled by N log N."""
+    import math
+    from oracle import oracle as O
+    f = O.init_f((128, 128, 128))
+    t = time.perf_counter()
+    O.solve(f)
+    t128 = time.perf_counter() - t
+    N = n[0] * n[1] * n[2]
+    for m in (512, 384, 256, 192, 128, 96, 64):
+        M = m ** 3
+        if M > N:
+            continue
+        est = t128 * (M / 128 ** 3) * (math.log(M) / math.log(128 ** 3))
+        if est * steps <= budget_s:
+            return (m, m, m) if M < N else tuple(n)
+    return (64, 64, 64)
+
+
 def run_reference(args):
+    """The reference's algorithm on the host cores: each step one oracle
+    solve (ParisPencil's FFT solve restated in C++/OpenMP) of a sample grid
+    sized so that the whole run stays within a few minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n = args.grid
-    N = n[0] * n[1] * n[2]
-    times, cores = oracle_baseline(n, steps=args.steps, warmup=args.warmup)
+    sample = reference_sample_grid(args.grid, args.steps + args.warmup)
+    N = sample[0] * sample[1] * sample[2]
+    times, cores = oracle_baseline(sample, steps=args.steps, warmup=args.warmup)
     total = sum(times)
     value = N * args.steps / total
     line = {
@@ -212,10 +236,11 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: analytic f of FishFry.hpp:22-44 on the reference grid",
-        "config": {"workload": "%dx%dx%d FP64 Poisson solve" % tuple(n), "grid": list(n), "precision": "fp64",
-                   "parallelism": "host threads"},
+        "config": {"workload": "%dx%dx%d FP64 Poisson solve" % tuple(args.grid), "grid": list(args.grid),
+                   "precision": "fp64", "parallelism": "host threads", "sample_grid": list(sample)},
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port",
-                         "sample": "%d full %dx%dx%d solves on %s" % (args.steps, *n, cpu_info() or "host")},
+                         "sample": "%d solves of a %dx%dx%d sample grid on %s" % (args.steps, *sample,
+                                                                                cpu_info() or "host")},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference has no CPU code path; this is the oracle's OpenMP restatement of its algorithm",
     }
@@ -285,40 +310,64 @@ def run_ours(args):
     # correctness of the last solve (outside timing)
     norms = ff.rel_norms(n, p, None, prec)
 
-    # end to end through the public API with host buffers: pinned f -> device,
-    # solve, phi -> pinned host, every step
+    # end to end through the public API with host buffers: every step copies
+    # its f from pinned host memory to the device, solves, and copies phi back
+    # to pinned host memory.  Steps are pipelined over two buffer sets: the
+    # input copy of step s+1 and the output copy of step s-1 run on their own
+    # streams while step s solves (PCIe is full duplex).
     e2e = None
     if not args.no_e2e:
         hf = torch.empty(N, dtype=dt, pin_memory=True)
-        hp = torch.empty(N, dtype=dt, pin_memory=True)
+        hp = [torch.empty(N, dtype=dt, pin_memory=True) for _ in range(2)]
         hf.copy_(f0.cpu())
-        for _ in range(2):
-            with torch.cuda.stream(stream):
-                d[:N].copy_(hf, non_blocking=True)
-            plan.solve(d, p, stream=stream)
-            with torch.cuda.stream(stream):
-                hp.copy_(p[:N], non_blocking=True)
-        stream.synchronize()
+        ref = p[:N].clone()                        # phi of the device-timed solves
+        dd = [d, torch.empty_like(d)]
+        pp = [p, torch.empty_like(p)]
+        s_in = torch.cuda.Stream(device=dev)
+        s_out = torch.cuda.Stream(device=dev)
+
+        def pipeline(nsteps):
+            loaded = [torch.cuda.Event() for _ in range(nsteps)]
+            solved = [torch.cuda.Event() for _ in range(nsteps)]
+            drained = [torch.cuda.Event() for _ in range(nsteps)]
+            for q in range(nsteps):
+                b = q % 2
+                with torch.cuda.stream(s_in):
+                    if q >= 2:
+                        s_in.wait_event(solved[q - 2])     # buffer set b free again
+                    dd[b][:N].copy_(hf, non_blocking=True)
+                    loaded[q].record(s_in)
+                stream.wait_event(loaded[q])
+                if q >= 2:
+                    stream.wait_event(drained[q - 2])      # phi of step q-2 read out
+                plan.solve(dd[b], pp[b], stream=stream)
+                solved[q].record(stream)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(solved[q])
+                    hp[b].copy_(pp[b][:N], non_blocking=True)
+                    drained[q].record(s_out)
+            return drained[nsteps - 1]
+
+        pipeline(2).synchronize()
         if world > 1:
             dist.barrier()
+        torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                d[:N].copy_(hf, non_blocking=True)
-            plan.solve(d, p, stream=stream)
-            with torch.cuda.stream(stream):
-                hp.copy_(p[:N], non_blocking=True)
-        e1.record(stream)
+        e0.record(s_in)
+        last = pipeline(args.steps)
+        s_out.wait_event(last)
+        e1.record(s_out)
         e1.synchronize()
         te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
         if world > 1:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e2e_ms = float(te.item())
+        same = bool(torch.equal(hp[(args.steps - 1) % 2].to(dev), ref))
         e2e = {"value": world * N * args.steps / (e2e_ms * 1e-3), "unit": "points/s",
                "h2d_bytes_per_step": N * esz, "d2h_bytes_per_step": N * esz,
-               "ms_per_step": e2e_ms / args.steps}
+               "ms_per_step": e2e_ms / args.steps, "pipelined": "two buffer sets, copies on their own streams",
+               "result_matches_device_timed_solve": same}
 
     if rank == 0:
         per_pass_bytes, total_bytes, five_pass_bytes = bytes_model(n, args.precision, nph)
@@ -572,8 +621,11 @@ def run_serve(args):
            ff.FF_FP32: torch.randn(512 ** 3, dtype=torch.float32, device=dev, generator=gen)}
     results = []
     for rate in args.rates:
+        t_rate = time.perf_counter()
         rng = np.random.default_rng(args.seed + int(rate))
         reqs = [(serve_dims(rng), int(rng.integers(2))) for _ in range(args.requests)]
+        print("serve rate %g: %d requests drawn in %.1f s" % (rate, len(reqs), time.perf_counter() - t_rate),
+              file=sys.stderr, flush=True)
         gaps = rng.exponential(1.0 / rate, args.requests)
         srv = ff.Server(int(args.budget_gb * 1e9), max_active=4096)
         # warm-up: every axis length's tables resident in both precisions
@@ -606,14 +658,17 @@ def run_serve(args):
         th = threading.Thread(target=producer)
         th.start()
         ready.wait()
-        for q in range(len(reqs)):
-            while ids[q] is None:
-                time.sleep(0.0002)
-            srv.wait(ids[q])
-            srv.release(ids[q])
+        # completions are taken in completion order and released at once (a
+        # finished request holds its buffers until released)
+        for _ in range(len(reqs)):
+            rid = srv.next()[0]
+            srv.release(rid)
         th.join()
         st = srv.stats()
         srv.close()
+        print("serve rate %g: %d requests in %.1f s, p50 %.3f ms, p99 %.3f ms, %.0f solves/s" % (
+            rate, st["completed"], time.perf_counter() - t_rate, st["p50_ms"], st["p99_ms"], st["solves_per_s"]),
+            file=sys.stderr, flush=True)
         results.append({"rate": rate, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
                         "max_ms": st["max_ms"], "solves_per_s": st["solves_per_s"],
                         "points_per_s": st["points_per_s"], "completed": st["completed"],

@@ -31,7 +31,8 @@ EXPORTS = [
     "ff_last_error", "ff_version",
     "ff_batch_create", "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
     "ff_batch_destroy",
-    "ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_fetch", "ff_server_release",
+    "ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_next", "ff_server_fetch",
+    "ff_server_release",
     "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy",
 ]
 
@@ -100,19 +101,21 @@ def _declare(L):
     L.ff_batch_bytes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
     L.ff_batch_solve.argtypes = [vp, pp, pp, vp, ctypes.POINTER(PhaseTimes)]
     L.ff_batch_tune.argtypes = [vp, pp, pp, vp, ctypes.c_int]
-    L.ff_batch_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
+    L.ff_batch_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip, ip]
     L.ff_batch_check.argtypes = [vp, vp]
     L.ff_batch_destroy.argtypes = [vp]
     L.ff_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.ff_server_submit.argtypes = [vp, i3, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]
     L.ff_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(RequestInfo)]
+    L.ff_server_next.argtypes = [vp, ctypes.c_double, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(RequestInfo)]
     L.ff_server_fetch.argtypes = [vp, ctypes.c_uint64, vp, ctypes.c_int]
     L.ff_server_release.argtypes = [vp, ctypes.c_uint64]
     L.ff_server_stats.argtypes = [vp, ctypes.POINTER(ServerReport)]
     L.ff_server_check.argtypes = [vp]
     L.ff_server_reset_stats.argtypes = [vp]
     L.ff_server_destroy.argtypes = [vp]
-    for name in ("ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_fetch", "ff_server_release",
+    for name in ("ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_next", "ff_server_fetch",
+                 "ff_server_release",
                  "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy"):
         getattr(L, name).restype = ctypes.c_int
     for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",

@@ -146,9 +146,11 @@ class Batch:
         check(lib().ff_batch_tune(self._h, d, p, _stream(stream), int(reps)), "ff_batch_tune")
 
     def shape(self, index, kind):
-        W, ct = ctypes.c_int(), ctypes.c_int()
-        check(lib().ff_batch_shape(self._h, int(index), int(kind), ctypes.byref(W), ctypes.byref(ct)), "ff_batch_shape")
-        return W.value, ct.value
+        """(W, ct, tma) of pass `kind` of grid `index`."""
+        W, ct, tma = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().ff_batch_shape(self._h, int(index), int(kind), ctypes.byref(W), ctypes.byref(ct),
+                                   ctypes.byref(tma)), "ff_batch_shape")
+        return W.value, ct.value, tma.value
 
     def check(self, stream=None):
         check(lib().ff_batch_check(self._h, _stream(stream)), "ff_batch_check")
@@ -197,6 +199,14 @@ class Server:
         info = _lib.RequestInfo()
         check(lib().ff_server_wait(self._h, int(rid), float(timeout_ms), ctypes.byref(info)), "ff_server_wait")
         return info.latency_ms, info.queue_ms, info.run_ms
+
+    def next(self, timeout_ms=-1.0):
+        """(id, latency, queue, run ms) of the next finished request (completion order)."""
+        rid = ctypes.c_uint64()
+        info = _lib.RequestInfo()
+        check(lib().ff_server_next(self._h, float(timeout_ms), ctypes.byref(rid), ctypes.byref(info)),
+              "ff_server_next")
+        return rid.value, info.latency_ms, info.queue_ms, info.run_ms
 
     def fetch(self, rid, out=None, on_host=None):
         """Copies the potential into `out` (device or host tensor; None: drop) and releases the request."""

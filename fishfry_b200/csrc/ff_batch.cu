@@ -55,6 +55,8 @@ struct ff_batch {
   void *desc = nullptr;          // device grid descriptors
   size_t desc_size = 0;
   unsigned char *desc_host = nullptr;   // pinned image of the descriptors
+  CUtensorMap *maps = nullptr;          // device: two tensor maps per grid (y, x boxes of its potential)
+  CUtensorMap *maps_host = nullptr;     // pinned image
   int2 *entries[5] = {};
   int *starts[5] = {};
   int ntiles[5] = {};
@@ -86,8 +88,9 @@ int pass_prepare(int precision, int kind, size_t smem, int *per_sm) {
 
 int pass_launch(const ff_batch *b, int kind, cudaStream_t st) {
   const BatchWork wl{b->entries[kind], b->starts[kind], b->count, b->tickets + kind};
-  return b->precision == FF_FP64 ? batch_pass_launch<double>(kind, b->desc, wl, b->blocks[kind], b->smem[kind], st)
-                                 : batch_pass_launch<float>(kind, b->desc, wl, b->blocks[kind], b->smem[kind], st);
+  return b->precision == FF_FP64
+             ? batch_pass_launch<double>(kind, b->desc, b->maps, wl, b->blocks[kind], b->smem[kind], st)
+             : batch_pass_launch<float>(kind, b->desc, b->maps, wl, b->blocks[kind], b->smem[kind], st);
 }
 
 }  // namespace
@@ -100,7 +103,9 @@ int batch_tiles_of(const BatchGridHost &g, int kind) {
     const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
     return (int)((npairs + s.W - 1) / s.W);
   }
-  const long ncols = (long)(kind == 2 ? g.n[1] : g.n[0]) * g.nh;
+  const long planes = kind == 2 ? g.n[1] : g.n[0];
+  if (s.tma) return (int)(planes * ((g.nh + s.W - 1) / s.W));
+  const long ncols = planes * g.nh;
   return (int)((ncols + s.W - 1) / s.W);
 }
 
@@ -114,6 +119,9 @@ bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const Ti
   if (kind != 0 && kind != 4) {
     const int w1 = 128 / (precision == FF_FP64 ? 16 : 8);
     if (s.W != w1 && s.W != 2 * w1 && s.W != 4 * w1) return false;
+    if (s.tma && s.W != w1) return false;
+  } else if (s.tma) {
+    return false;
   }
   return batch_shape_smem(precision, g, kind, s) <= kBatchSmem;
 }
@@ -123,19 +131,26 @@ bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const Ti
 // where the length has them.
 TileShape batch_default_shape(int precision, const BatchGridHost &g, int kind) {
   const int n = batch_axis_len(g, kind);
-  TileShape s{1, batch_special_n(n) ? 1 : 0};
+  TileShape s{1, batch_special_n(n) ? 1 : 0, 0};
   if (kind == 0 || kind == 4) {
     const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
     int W = std::max(1, 2048 / std::max(1, g.n[2]));
     W = (int)std::min<long>(W, npairs);
-    while (W > 1 && !batch_shape_valid(precision, g, kind, TileShape{W, s.ct})) W--;
+    while (W > 1 && !batch_shape_valid(precision, g, kind, TileShape{W, s.ct, 0})) W--;
     s.W = W;
     return s;
   }
   const int w1 = 128 / (precision == FF_FP64 ? 16 : 8);
+  // long lines with many columns per plane: one-plane tiles by TMA, as the
+  // single-grid passes
+  if (n >= 256 && g.nh >= 4 * w1) {
+    s.W = w1;
+    s.tma = 1;
+    return s;
+  }
   int W = w1;
   for (int m = 4; m >= 1; m /= 2) {
-    const TileShape t{m * w1, s.ct};
+    const TileShape t{m * w1, s.ct, 0};
     if (m * w1 * n <= 4096 && batch_shape_valid(precision, g, kind, t)) {
       W = m * w1;
       break;
@@ -204,6 +219,24 @@ void batch_grid_init(BatchGridHost &h, const int n[3], const double *lo, const d
   h.nh = h.n[2] / 2 + 1;
   h.nhp = precision == FF_FP64 ? h.nh : (h.nh + 1) & ~1;
   h.invN = 1.0 / (double(h.n[0]) * double(h.n[1]) * double(h.n[2]));
+  // TMA boxes: the largest divisor of the line length up to 256 rows
+  for (int x = 0; x < 2; x++) {
+    const int n = x == 0 ? h.n[1] : h.n[0];
+    int d = std::min(n, 256);
+    while (n % d) d--;
+    h.box_rows[x] = d;
+  }
+}
+
+int batch_grid_maps(const BatchGridHost &g, int precision, CUtensorMap maps[2]) {
+  const size_t esz = precision == FF_FP64 ? 8 : 4;
+  const int w1 = 128 / (int)(2 * esz);
+  for (int x = 0; x < 2; x++) {
+    const int rc = encode_spectrum_map(g.potential, g.n[0], g.n[1], g.nh, g.nhp, esz, w1, g.box_rows[x], x == 1,
+                                       &maps[x]);
+    if (rc != FF_OK) return rc;
+  }
+  return FF_OK;
 }
 
 size_t batch_grid_bytes(const BatchGridHost &h, int precision) {
@@ -313,8 +346,13 @@ int set_buffers(ff_batch *b, void *const *density, void *const *potential) {
 
 int upload_desc(ff_batch *b, cudaStream_t st) {
   if (!b->desc_dirty) return FF_OK;
-  for (int g = 0; g < b->count; g++) desc_fill(b->precision, b->desc_host + g * b->desc_size, b->grids[g]);
+  for (int g = 0; g < b->count; g++) {
+    desc_fill(b->precision, b->desc_host + g * b->desc_size, b->grids[g]);
+    const int rc = batch_grid_maps(b->grids[g], b->precision, b->maps_host + 2 * g);
+    if (rc != FF_OK) return rc;
+  }
   FF_CUDA(cudaMemcpyAsync(b->desc, b->desc_host, b->count * b->desc_size, cudaMemcpyHostToDevice, st));
+  FF_CUDA(cudaMemcpyAsync(b->maps, b->maps_host, 2 * b->count * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
   // the pinned image may be rewritten by the next call only after this copy
   FF_CUDA(cudaStreamSynchronize(st));
   b->desc_dirty = false;
@@ -390,6 +428,7 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
   const size_t o_status = take(sizeof(int));
   const size_t o_tickets = take(5 * sizeof(int));
   const size_t o_desc = take((size_t)count * b->desc_size);
+  const size_t o_maps = take((size_t)count * 2 * sizeof(CUtensorMap));
   size_t o_ent[5], o_start[5];
   for (int k = 0; k < 5; k++) {
     o_ent[k] = take((size_t)count * sizeof(int2));
@@ -401,8 +440,10 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
     delete b;
     return set_error(FF_ERR_NOMEM, "ff_batch_create: cudaMalloc(%zu) for tables failed", off);
   }
-  if (cudaMallocHost((void **)&b->desc_host, (size_t)count * b->desc_size) != cudaSuccess) {
+  if (cudaMallocHost((void **)&b->desc_host, (size_t)count * b->desc_size) != cudaSuccess ||
+      cudaMallocHost((void **)&b->maps_host, (size_t)count * 2 * sizeof(CUtensorMap)) != cudaSuccess) {
     cudaGetLastError();
+    if (b->desc_host) cudaFreeHost(b->desc_host);
     cudaFree(b->dmem);
     delete b;
     return set_error(FF_ERR_NOMEM, "ff_batch_create: pinned descriptor image");
@@ -411,6 +452,7 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
   b->status = reinterpret_cast<int *>(base + o_status);
   b->tickets = reinterpret_cast<int *>(base + o_tickets);
   b->desc = base + o_desc;
+  b->maps = reinterpret_cast<CUtensorMap *>(base + o_maps);
   for (int k = 0; k < 5; k++) {
     b->entries[k] = reinterpret_cast<int2 *>(base + o_ent[k]);
     b->starts[k] = reinterpret_cast<int *>(base + o_start[k]);
@@ -459,11 +501,12 @@ int ff_batch_bytes(const ff_batch *b, int index, size_t *bytes) {
   return FF_OK;
 }
 
-int ff_batch_shape(const ff_batch *b, int index, int kind, int *W, int *ct) {
+int ff_batch_shape(const ff_batch *b, int index, int kind, int *W, int *ct, int *tma) {
   if (!b || index < 0 || index >= b->count || kind < 0 || kind > 4)
     return set_error(FF_ERR_INVALID, "ff_batch_shape: bad argument");
   if (W) *W = b->grids[index].shape[kind].W;
   if (ct) *ct = b->grids[index].shape[kind].ct;
+  if (tma) *tma = b->grids[index].shape[kind].tma;
   return FF_OK;
 }
 
@@ -528,10 +571,11 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
       const TileShape d = batch_default_shape(b->precision, ref, k);
       for (int ct = batch_special_n(n) ? 1 : 0; ct >= 0; ct--) {
         if (k == 0 || k == 4) {
-          for (int W : {std::max(1, d.W / 2), d.W, d.W * 2}) cand.push_back(TileShape{W, ct});
+          for (int W : {std::max(1, d.W / 2), d.W, d.W * 2}) cand.push_back(TileShape{W, ct, 0});
         } else {
           const int w1 = 128 / (int)b->csz;
-          for (int m : {1, 2, 4}) cand.push_back(TileShape{m * w1, ct});
+          for (int m : {1, 2, 4}) cand.push_back(TileShape{m * w1, ct, 0});
+          cand.push_back(TileShape{w1, ct, 1});
         }
       }
       TileShape best = ref.shape[k];
@@ -572,6 +616,7 @@ int ff_batch_destroy(ff_batch *b) {
     if (b->ev[e]) cudaEventDestroy(b->ev[e]);
   if (b->cap) cudaStreamDestroy(b->cap);
   if (b->desc_host) cudaFreeHost(b->desc_host);
+  if (b->maps_host) cudaFreeHost(b->maps_host);
   int rc = FF_OK;
   if (b->dmem && cudaFree(b->dmem) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_destroy: cudaFree failed");
   delete b;

@@ -8,6 +8,7 @@
 // take tiles from a ticket counter until the work list is exhausted.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <vector_types.h>
 
@@ -24,6 +25,9 @@ constexpr size_t kBatchSmem = 72 * 1024;
 // Axis lengths with compile-time specialised batch tiles; others use the
 // runtime plan of their axis.
 #define FF_FOR_EACH_BATCH_N(X) X(32) X(48) X(64) X(80) X(96) X(128) X(256) X(512)
+
+// Lengths with compile-time specialised one-plane TMA tiles.
+#define FF_FOR_EACH_BATCH_TMA_N(X) X(256) X(512)
 
 inline bool batch_special_n(int n) {
 #define FF_CASE(NN) if (n == NN) return true;
@@ -46,9 +50,13 @@ struct BatchWork {
 // strided passes take W columns (W * sizeof(complex) a multiple of 128
 // bytes: 1, 2 or 4 rows of 128 bytes).  ct = 1 selects the compile-time
 // specialised tile for the axis length (batch_special_n), 0 the runtime plan.
+// tma = 1 (strided passes only, W = 128 bytes of columns): the tile is W kh
+// columns of one plane, loaded by TMA boxes as in the single-grid passes;
+// tma = 0: W columns of the flattened (plane, kh) index, read straight from HBM.
 struct TileShape {
   int W;
   int ct;
+  int tma;
 };
 
 // Shared memory of one tile (bytes, with alignment slack).
@@ -64,8 +72,11 @@ inline size_t batch_tile_smem(int kind, int n_axis, int nk, int nhp, int W, size
 
 // Launches pass `kind` (0..4) of the precision-T batch kernel; grids points
 // at the device array of the batch's grid descriptors.
+// maps: per grid two tensor maps of its potential's half spectrum (y boxes,
+// x boxes), used by tiles with tma = 1.
 template <typename T>
-int batch_pass_launch(int kind, const void *grids, const BatchWork &wl, int blocks, size_t smem, cudaStream_t st);
+int batch_pass_launch(int kind, const void *grids, const CUtensorMap *maps, const BatchWork &wl, int blocks,
+                      size_t smem, cudaStream_t st);
 // Raises the pass kernel's shared-memory limit to kBatchSmem and reports how
 // many blocks of `smem` bytes fit on one SM.
 template <typename T> int batch_pass_prepare(int kind, size_t smem, int *per_sm);
@@ -86,7 +97,14 @@ struct BatchGridHost {
   int *status;
   void *density, *potential;
   TileShape shape[5];
+  int box_rows[2];   // rows per TMA box of the y and x passes
 };
+
+// Tensor map of a half spectrum (ff_solve.cu).
+int encode_spectrum_map(void *base, int ni, int nj, int nh, int nhp, size_t esz, int W, int box_rows, bool xpass,
+                        CUtensorMap *map);
+// The two tensor maps (y boxes, x boxes) of a grid's potential.
+int batch_grid_maps(const BatchGridHost &g, int precision, CUtensorMap maps[2]);
 
 // Host helpers shared by the batch and the server (ff_batch.cu).
 int batch_axis_len(const BatchGridHost &g, int kind);

@@ -21,6 +21,7 @@ template <typename T> struct alignas(16) GridDesc {
   T *density;
   T *potential;
   TileShape shape[5];
+  int box_rows[2];   // rows per TMA box: y pass, x pass
 };
 
 // ------------------------------------------------------------ column tiles
@@ -127,9 +128,32 @@ __device__ __forceinline__ void cols_tile_w(int wb, const PassArgs<T> &a, const 
 // One tile of pass KIND of grid descriptor g.  Returns false if a bounded
 // wait gave up (the status word is set).  parity tracks the block's
 // mbarrier phase across the inbound bulk copies of the z inverse tiles.
+// Strided tile of one plane by TMA (the single-grid tile code): W = 128
+// bytes of kh columns, all n rows; tile = plane * ktiles + kt.
+template <typename T, bool XPASS, bool INV, int N>
+__device__ __forceinline__ bool tma_cols_tile(const GridDesc<T> &g, const CUtensorMap *map, int tile,
+                                              typename Cplx<T>::type *sm, uint64_t *mbar, uint32_t &parity) {
+  using C = typename Cplx<T>::type;
+  constexpr int W = 128 / (int)sizeof(C);
+  const PassArgs<T> &a = g.a;
+  const int n = XPASS ? a.ni : a.nj;
+  const int ktiles = (a.nh + W - 1) / W;
+  const int o = tile / ktiles, kt = tile - o * ktiles;
+  const int box_rows = g.box_rows[XPASS ? 1 : 0];
+  if (!tma_tile<C, W, XPASS>(map, sm, mbar, parity, n, box_rows, o, kt, a.status)) return false;
+  parity ^= 1u;
+  if constexpr (XPASS) {
+    x_tile<T, W, N>(map, a, o, kt, box_rows, sm);
+  } else {
+    PointTile<W, C> t{sm};
+    y_tile<T, W, INV, N>(t, reinterpret_cast<C *>(INV ? g.density : g.potential), a, o, kt, sm);
+  }
+  return true;
+}
+
 template <typename T, int KIND>
-__device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, int tile, typename Cplx<T>::type *sm,
-                                           uint64_t *mbar, uint32_t &parity) {
+__device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorMap *maps, int tile,
+                                           typename Cplx<T>::type *sm, uint64_t *mbar, uint32_t &parity) {
   using C = typename Cplx<T>::type;
   const PassArgs<T> &a = g.a;
   const TileShape sh = g.shape[KIND];
@@ -176,6 +200,19 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, int tile, typen
     C *dst = reinterpret_cast<C *>(KIND == 3 ? g.density : g.potential);
     const int wb = sh.W * (int)sizeof(C) / 128;
     const int n = XPASS ? a.ni : a.nj;
+    if (sh.tma) {
+      const CUtensorMap *map = maps + (XPASS ? 1 : 0);
+      if (sh.ct) {
+        switch (n) {
+#define FF_CASE(NN) \
+  case NN: return tma_cols_tile<T, XPASS, INV, NN>(g, map, tile, sm, mbar, parity);
+          FF_FOR_EACH_BATCH_TMA_N(FF_CASE)
+#undef FF_CASE
+          default: break;
+        }
+      }
+      return tma_cols_tile<T, XPASS, INV, 0>(g, map, tile, sm, mbar, parity);
+    }
     if (sh.ct) {
       switch (n) {
 #define FF_CASE(NN) \
@@ -192,8 +229,12 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, int tile, typen
 
 // Persistent pass kernel: blocks take tiles by ticket until the work list is
 // exhausted; the tile's grid is found by binary search over the prefix sums.
+#ifndef FF_BATCH_MINB
+#define FF_BATCH_MINB 3
+#endif
 template <typename T, int KIND>
-__global__ void __launch_bounds__(kZThreads, 3) k_batch(const GridDesc<T> *__restrict__ grids, const BatchWork wl) {
+__global__ void __launch_bounds__(kZThreads, (KIND == 0 || KIND == 4) ? FF_BATCH_MINB : 3)
+    k_batch(const GridDesc<T> *__restrict__ grids, const CUtensorMap *__restrict__ maps, const BatchWork wl) {
   using C = typename Cplx<T>::type;
   extern __shared__ unsigned char smraw[];
   __shared__ __align__(8) uint64_t mbar;
@@ -222,6 +263,30 @@ __global__ void __launch_bounds__(kZThreads, 3) k_batch(const GridDesc<T> *__res
       else hi = mid - 1;
     }
     const int g = wl.entry[lo].x;
+    if constexpr (KIND == 0) {
+      // the forward z pass reads its lines with thread loads: hint the lines
+      // of the tile claimed about one round later (ticket t + gridDim.x) into L2
+      const int t2 = t + (int)gridDim.x;
+      if (threadIdx.x == 0 && t2 < total) {
+        int a2 = lo, b2 = wl.nentry - 1;
+        while (a2 < b2) {
+          const int mid = (a2 + b2 + 1) >> 1;
+          if (__ldg(wl.start + mid) <= t2) a2 = mid;
+          else b2 = mid - 1;
+        }
+        const GridDesc<T> *G = grids + wl.entry[a2].x;
+        const int zW = G->shape[0].W;
+        const int nk = G->a.nk;
+        const long nlines = (long)G->a.ni * G->a.nj;
+        const long l0 = (long)(t2 - __ldg(wl.start + a2)) * 2 * zW;
+        const long l1 = min(l0 + 2 * zW, nlines);
+        // within the buffer: its size is max(real field, half spectrum)
+        const size_t cap = max((size_t)nlines * nk * sizeof(T), (size_t)nlines * G->a.nhp * 2 * sizeof(T));
+        const size_t b0 = ((size_t)l0 * nk * sizeof(T)) & ~size_t(15);
+        const size_t b1 = min(((size_t)l1 * nk * sizeof(T) + 15) & ~size_t(15), cap & ~size_t(15));
+        if (b1 > b0) l2_prefetch(reinterpret_cast<const char *>(G->density) + b0, (uint32_t)(b1 - b0));
+      }
+    }
     if (g != last_g) {
       // descriptor of the tile's grid into shared memory (read-only below)
       const int4 *s = reinterpret_cast<const int4 *>(grids + g);
@@ -230,7 +295,7 @@ __global__ void __launch_bounds__(kZThreads, 3) k_batch(const GridDesc<T> *__res
       __syncthreads();
       last_g = g;
     }
-    if (!batch_tile<T, KIND>(s_desc, t - __ldg(wl.start + lo), sm, &mbar, parity)) break;
+    if (!batch_tile<T, KIND>(s_desc, maps + 2 * g, t - __ldg(wl.start + lo), sm, &mbar, parity)) break;
   }
 }
 
@@ -247,14 +312,15 @@ template <typename T> static void *batch_kernel(int kind) {
 }
 
 template <typename T>
-int batch_pass_launch(int kind, const void *grids, const BatchWork &wl, int blocks, size_t smem, cudaStream_t st) {
+int batch_pass_launch(int kind, const void *grids, const CUtensorMap *maps, const BatchWork &wl, int blocks,
+                      size_t smem, cudaStream_t st) {
   const GridDesc<T> *g = static_cast<const GridDesc<T> *>(grids);
   switch (kind) {
-    case 0: k_batch<T, 0><<<blocks, kZThreads, smem, st>>>(g, wl); break;
-    case 1: k_batch<T, 1><<<blocks, kZThreads, smem, st>>>(g, wl); break;
-    case 2: k_batch<T, 2><<<blocks, kZThreads, smem, st>>>(g, wl); break;
-    case 3: k_batch<T, 3><<<blocks, kZThreads, smem, st>>>(g, wl); break;
-    default: k_batch<T, 4><<<blocks, kZThreads, smem, st>>>(g, wl); break;
+    case 0: k_batch<T, 0><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
+    case 1: k_batch<T, 1><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
+    case 2: k_batch<T, 2><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
+    case 3: k_batch<T, 3><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
+    default: k_batch<T, 4><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
   }
   FF_CUDA(cudaGetLastError());
   return FF_OK;
@@ -293,11 +359,14 @@ template <typename T> void batch_desc_fill(void *dst, const BatchGridHost &h) {
   g.density = static_cast<T *>(h.density);
   g.potential = static_cast<T *>(h.potential);
   for (int k = 0; k < 5; k++) g.shape[k] = h.shape[k];
+  g.box_rows[0] = h.box_rows[0];
+  g.box_rows[1] = h.box_rows[1];
   memcpy(dst, &g, sizeof(g));
 }
 
 #define FF_INSTANTIATE_BATCH(T)                                                                               \
-  template int batch_pass_launch<T>(int, const void *, const BatchWork &, int, size_t, cudaStream_t);        \
+  template int batch_pass_launch<T>(int, const void *, const CUtensorMap *, const BatchWork &, int, size_t,   \
+                                    cudaStream_t);                                                          \
   template int batch_pass_prepare<T>(int, size_t, int *);                                                    \
   template size_t batch_desc_size<T>();                                                                      \
   template void batch_desc_fill<T>(void *, const BatchGridHost &);

@@ -115,6 +115,8 @@ struct Lane {
   cudaStream_t stream = nullptr;
   void *desc = nullptr;                    // device descriptors [slots]
   unsigned char *desc_host = nullptr;      // pinned image
+  CUtensorMap *maps = nullptr;             // device tensor maps [slots][2] (y, x boxes of the potential)
+  CUtensorMap *maps_host = nullptr;        // pinned image
   std::vector<int> free_slots;
   // ring buffers: per step r and kind k: entries [slots] int2, starts [slots + 1] int, 5 tickets
   void *ring_dev = nullptr;
@@ -149,6 +151,9 @@ struct ff_server {
   std::map<std::pair<int, int>, AxisEntry> axes;   // (n, precision)
   std::map<uint64_t, Request> reqs;
   std::deque<uint64_t> pending;
+  std::vector<uint64_t> active;   // admitted, not yet done (loading or running)
+  std::deque<uint64_t> finished;  // done, not yet claimed by ff_server_next
+  bool admit_dirty = false;       // memory or slots freed, or requests arrived, since the last admission pass
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::thread worker;
@@ -174,19 +179,6 @@ size_t step_block_bytes(int slots) {
   return 5 * (r(slots * sizeof(int2)) + r((slots + 1) * sizeof(int))) + r(5 * sizeof(int));
 }
 
-void step_layout(const Lane &L, int slots, int r, bool dev, int2 **ent, int **start, int **tickets) {
-  auto rr = [](size_t b) { return (b + 255) & ~size_t(255); };
-  char *base = (dev ? static_cast<char *>(L.ring_dev) : reinterpret_cast<char *>(L.ring_host)) + r * L.ring_bytes;
-  size_t off = 0;
-  for (int k = 0; k < 5; k++) {
-    ent[k] = reinterpret_cast<int2 *>(base + off);
-    off += rr(slots * sizeof(int2));
-    start[k] = reinterpret_cast<int *>(base + off);
-    off += rr((slots + 1) * sizeof(int));
-  }
-  *tickets = reinterpret_cast<int *>(base + off);
-}
-
 int lane_init(ff_server *s, Lane &L, int precision) {
   const int slots = s->cfg.max_active;
   L.precision = precision;
@@ -194,6 +186,8 @@ int lane_init(ff_server *s, Lane &L, int precision) {
   FF_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
   FF_CUDA(cudaMalloc(&L.desc, slots * L.dsz));
   FF_CUDA(cudaMallocHost((void **)&L.desc_host, slots * L.dsz));
+  FF_CUDA(cudaMalloc((void **)&L.maps, (size_t)slots * 2 * sizeof(CUtensorMap)));
+  FF_CUDA(cudaMallocHost((void **)&L.maps_host, (size_t)slots * 2 * sizeof(CUtensorMap)));
   L.ring_bytes = step_block_bytes(slots);
   FF_CUDA(cudaMalloc(&L.ring_dev, kRing * L.ring_bytes));
   FF_CUDA(cudaMallocHost((void **)&L.ring_host, kRing * L.ring_bytes));
@@ -214,6 +208,8 @@ void lane_free(Lane &L) {
   if (L.ring_host) cudaFreeHost(L.ring_host);
   if (L.ring_dev) cudaFree(L.ring_dev);
   if (L.desc_host) cudaFreeHost(L.desc_host);
+  if (L.maps_host) cudaFreeHost(L.maps_host);
+  if (L.maps) cudaFree(L.maps);
   if (L.desc) cudaFree(L.desc);
   if (L.stream) cudaStreamDestroy(L.stream);
 }
@@ -243,9 +239,14 @@ void fail(ff_server *s, int rc) {
 }
 
 // Admission of pending requests in arrival order; a request that does not
-// fit now is passed over (later, smaller ones may fit) and retried next round.
+// fit now is passed over (later, smaller ones may fit) and retried when
+// memory or slots are freed.  At most kAdmitWindow queued requests are
+// examined per pass, so a long queue costs nothing while the budget is full.
+constexpr int kAdmitWindow = 64;
+
 int admit(ff_server *s) {
-  for (auto it = s->pending.begin(); it != s->pending.end();) {
+  int seen = 0;
+  for (auto it = s->pending.begin(); it != s->pending.end() && seen < kAdmitWindow; seen++) {
     Request &q = s->reqs[*it];
     Lane &L = s->lane[q.precision == FF_FP64 ? 0 : 1];
     size_t od = 0, op = 0;
@@ -288,6 +289,7 @@ int admit(ff_server *s) {
     FF_CUDA(cudaEventRecord(q.in_ev, s->copy));
     q.state = kLoading;
     q.t_admit = Clock::now();
+    s->active.push_back(q.id);
     it = s->pending.erase(it);
   }
   return FF_OK;
@@ -305,18 +307,28 @@ int issue_step(ff_server *s, Lane &L, bool *issued) {
     }
   if (r < 0) return FF_OK;
   std::vector<uint64_t> members;
-  for (auto &kv : s->reqs) {
-    Request &q = kv.second;
+  for (uint64_t id : s->active) {
+    Request &q = s->reqs[id];
     if (q.state == kRunning && q.precision == L.precision && q.next_pass < 5) members.push_back(q.id);
   }
   if (members.empty()) return FF_OK;
-  const int slots = s->cfg.max_active;
-  int2 *ent_h[5], *ent_d[5];
-  int *st_h[5], *st_d[5], *tk_h, *tk_d;
-  step_layout(L, slots, r, false, ent_h, st_h, &tk_h);
-  step_layout(L, slots, r, true, ent_d, st_d, &tk_d);
+  // compact layout of this step's work lists in ring block r: per kind the
+  // entries (int2) and the prefix sums (int), then the five tickets
   int cnt[5] = {0, 0, 0, 0, 0};
-  for (int k = 0; k < 5; k++) st_h[k][0] = 0;
+  for (uint64_t id : members) cnt[s->reqs[id].next_pass]++;
+  size_t e_off[5], s_off[5], off = 0;
+  for (int k = 0; k < 5; k++) {
+    e_off[k] = off;
+    off += cnt[k] * sizeof(int2);
+    s_off[k] = off;
+    off += ((cnt[k] + 1) * sizeof(int) + 7) & ~size_t(7);
+  }
+  const size_t t_off = off;
+  off += 5 * sizeof(int);
+  unsigned char *hb = L.ring_host + (size_t)r * L.ring_bytes;
+  char *db = static_cast<char *>(L.ring_dev) + (size_t)r * L.ring_bytes;
+  int fill[5] = {0, 0, 0, 0, 0};
+  for (int k = 0; k < 5; k++) reinterpret_cast<int *>(hb + s_off[k])[0] = 0;
   for (uint64_t id : members) {
     Request &q = s->reqs[id];
     if (!q.desc_uploaded) {
@@ -325,24 +337,31 @@ int issue_step(ff_server *s, Lane &L, bool *issued) {
       else batch_desc_fill<float>(img, q.g);
       FF_CUDA(cudaMemcpyAsync(static_cast<char *>(L.desc) + (size_t)q.slot * L.dsz, img, L.dsz,
                               cudaMemcpyHostToDevice, L.stream));
+      CUtensorMap *mh = L.maps_host + 2 * (size_t)q.slot;
+      const int rc = batch_grid_maps(q.g, q.precision, mh);
+      if (rc != FF_OK) return rc;
+      FF_CUDA(cudaMemcpyAsync(L.maps + 2 * (size_t)q.slot, mh, 2 * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                              L.stream));
       q.desc_uploaded = true;
     }
     const int k = q.next_pass;
-    ent_h[k][cnt[k]] = make_int2(q.slot, k);
-    st_h[k][cnt[k] + 1] = st_h[k][cnt[k]] + batch_tiles_of(q.g, k);
-    cnt[k]++;
+    int *st = reinterpret_cast<int *>(hb + s_off[k]);
+    reinterpret_cast<int2 *>(hb + e_off[k])[fill[k]] = make_int2(q.slot, k);
+    st[fill[k] + 1] = st[fill[k]] + batch_tiles_of(q.g, k);
+    fill[k]++;
     q.next_pass++;
     if (q.next_pass == 5) q.finish_step = L.next_step;
   }
-  for (int k = 0; k < 5; k++) tk_h[k] = 0;
-  FF_CUDA(cudaMemcpyAsync(ent_d[0], ent_h[0], L.ring_bytes, cudaMemcpyHostToDevice, L.stream));
+  std::memset(hb + t_off, 0, 5 * sizeof(int));
+  FF_CUDA(cudaMemcpyAsync(db, hb, off, cudaMemcpyHostToDevice, L.stream));
   for (int k = 0; k < 5; k++) {
     if (!cnt[k]) continue;
-    const BatchWork wl{ent_d[k], st_d[k], cnt[k], tk_d + k};
-    const int tiles = st_h[k][cnt[k]];
+    const BatchWork wl{reinterpret_cast<const int2 *>(db + e_off[k]), reinterpret_cast<const int *>(db + s_off[k]),
+                       cnt[k], reinterpret_cast<int *>(db + t_off) + k};
+    const int tiles = reinterpret_cast<int *>(hb + s_off[k])[cnt[k]];
     const int blocks = std::max(1, std::min(tiles, 3 * s->num_sms));
-    int rc = L.precision == FF_FP64 ? batch_pass_launch<double>(k, L.desc, wl, blocks, kBatchSmem, L.stream)
-                                    : batch_pass_launch<float>(k, L.desc, wl, blocks, kBatchSmem, L.stream);
+    int rc = L.precision == FF_FP64 ? batch_pass_launch<double>(k, L.desc, L.maps, wl, blocks, kBatchSmem, L.stream)
+                                    : batch_pass_launch<float>(k, L.desc, L.maps, wl, blocks, kBatchSmem, L.stream);
     if (rc != FF_OK) return rc;
     s->launches++;
   }
@@ -375,8 +394,10 @@ int retire_steps(ff_server *s, Lane &L, bool *progress) {
       if (it == s->reqs.end()) continue;
       Request &q = it->second;
       if (q.finish_step == oldest && q.state == kRunning) {
+        s->active.erase(std::find(s->active.begin(), s->active.end(), id));
         q.state = kDone;
         q.t_done = now;
+        s->finished.push_back(id);
         s->completed++;
         s->lat_ms.push_back(ms_between(q.t_submit, q.t_done));
         s->points_done += double(q.n[0]) * q.n[1] * q.n[2];
@@ -397,10 +418,13 @@ void scheduler(ff_server *s) {
     int rc = FF_OK;
     for (int l = 0; l < 2 && rc == FF_OK; l++) rc = retire_steps(s, s->lane[l], &progress);
     if (progress) s->cv_done.notify_all();
-    if (rc == FF_OK && !s->pending.empty()) rc = admit(s);
+    if (rc == FF_OK && !s->pending.empty() && s->admit_dirty) {
+      s->admit_dirty = false;
+      rc = admit(s);
+    }
     if (rc == FF_OK) {
-      for (auto &kv : s->reqs) {
-        Request &q = kv.second;
+      for (uint64_t id : s->active) {
+        Request &q = s->reqs[id];
         if (q.state != kLoading) continue;
         const cudaError_t e = cudaEventQuery(q.in_ev);
         if (e == cudaSuccess) {
@@ -417,14 +441,8 @@ void scheduler(ff_server *s) {
       rc = issue_step(s, s->lane[l], &issued);
       progress = progress || issued;
     }
-    int active = 0;
-    bool busy = false;
-    for (auto &kv : s->reqs)
-      if (kv.second.state == kLoading || kv.second.state == kRunning) {
-        active++;
-        busy = true;
-      }
-    s->max_active_seen = std::max(s->max_active_seen, active);
+    const bool busy = !s->active.empty();
+    s->max_active_seen = std::max(s->max_active_seen, (int)s->active.size());
     if (rc != FF_OK) {
       fail(s, rc);
       s->cv_done.notify_all();
@@ -507,6 +525,7 @@ int ff_server_submit(ff_server *s, const int n[3], int precision, const void *f,
     s->submitted++;
     s->reqs.emplace(q.id, q);
     s->pending.push_back(q.id);
+    s->admit_dirty = true;
   }
   s->cv_work.notify_one();
   return FF_OK;
@@ -532,6 +551,33 @@ int ff_server_wait(ff_server *s, uint64_t id, double timeout_ms, ff_request_info
     if (s->fatal != FF_OK) return set_error(s->fatal, "ff_server_wait: server stopped: %s", s->fatal_msg);
     if (timeout_ms >= 0 && Clock::now() >= deadline)
       return set_error(FF_ERR_TIMEOUT, "ff_server_wait: request %llu not done", (unsigned long long)id);
+    if (timeout_ms >= 0) s->cv_done.wait_until(lk, deadline);
+    else s->cv_done.wait(lk);
+  }
+}
+
+int ff_server_next(ff_server *s, double timeout_ms, uint64_t *id, ff_request_info *info) {
+  if (!s || !id) return set_error(FF_ERR_INVALID, "ff_server_next: null argument");
+  std::unique_lock<std::mutex> lk(s->mu);
+  const auto deadline = Clock::now() + std::chrono::microseconds((long long)(timeout_ms * 1000.0));
+  for (;;) {
+    while (!s->finished.empty()) {
+      const uint64_t q = s->finished.front();
+      s->finished.pop_front();
+      auto it = s->reqs.find(q);
+      if (it == s->reqs.end()) continue;   // already released
+      *id = q;
+      if (info) {
+        const Request &r = it->second;
+        info->latency_ms = ms_between(r.t_submit, r.t_done);
+        info->queue_ms = ms_between(r.t_submit, r.t_admit);
+        info->run_ms = ms_between(r.t_admit, r.t_done);
+      }
+      return FF_OK;
+    }
+    if (s->fatal != FF_OK) return set_error(s->fatal, "ff_server_next: server stopped: %s", s->fatal_msg);
+    if (timeout_ms >= 0 && Clock::now() >= deadline)
+      return set_error(FF_ERR_TIMEOUT, "ff_server_next: no request finished");
     if (timeout_ms >= 0) s->cv_done.wait_until(lk, deadline);
     else s->cv_done.wait(lk);
   }
@@ -572,6 +618,7 @@ int ff_server_release(ff_server *s, uint64_t id) {
     s->arena.release(q.off_d, q.bytes);
     s->arena.release(q.off_p, q.bytes);
     s->lane[q.precision == FF_FP64 ? 0 : 1].free_slots.push_back(q.slot);
+    s->admit_dirty = true;
   }
   if (q.in_ev) cudaEventDestroy(q.in_ev);
   s->reqs.erase(it);

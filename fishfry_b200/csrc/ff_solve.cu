@@ -37,125 +37,6 @@ namespace ff {
 // every other length runs the same kernels with the plan read at run time.
 #define FF_FOR_EACH_SPECIAL_N(X) X(256) X(512) X(1024)
 
-// --------------------------------------------------------- strided tiles
-// A strided tile is W consecutive kh columns (128-byte rows) of all n rows of
-// one plane, held point-major: y tiles are (plane i, rows j), x tiles are
-// (plane j, rows i).
-
-// y transform of one tile; stage 0 reads through ld0 (the TMA-filled tile or
-// HBM/L2 directly), the last stage stores from registers straight to HBM at
-// the digit-reversed rows.
-template <typename T, int W, bool INV, int N, typename LD0>
-__device__ __forceinline__ void y_tile(LD0 &ld0, typename Cplx<T>::type *dst, const PassArgs<T> &a, int o, int kt,
-                                       typename Cplx<T>::type *sm) {
-  using C = typename Cplx<T>::type;
-  const AxisDev<C> &ax = a.ax[1];
-  const int kh0 = kt * W;
-  const int ncol = min(W, a.nh - kh0);
-  const long base = (long)o * a.nj * a.nhp + kh0;
-  const int pitch = a.nhp;
-  const auto rl = rev_last<N>(ax);
-  PointTile<W, C> tile{sm};
-  auto gst = [&](int pos, int c, C v) {
-    if (c < ncol) dst[base + (long)rl(pos) * pitch + c] = v;
-  };
-    dif_all<N, INV, Map::ColFast, W, kZThreads, false, (sizeof(T) == 8)>(ax, ld0, tile, gst, W);
-}
-
-// x transform of one TMA-filled tile: forward, filter, inverse.  The inverse
-// ends in natural order in place, so the finished tile leaves by TMA stores
-// of the same boxes it came in with (columns past nh are clipped).
-template <typename T, int W, int N>
-__device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T> &a, int j, int kt, int box_rows,
-                                       typename Cplx<T>::type *sm) {
-  using C = typename Cplx<T>::type;
-  constexpr int NT = kZThreads;
-  // FP64: twiddle powers by recurrence (fewer table loads); FP32: table loads
-  // (FP64-generated values), keeping the FP64 pipe for the filter
-  constexpr bool TWX = sizeof(T) == 8;
-  const AxisDev<C> &ax = a.ax[0];
-  const int n = N > 0 ? N : ax.n;
-  const int kh0 = kt * W;
-  const int ncol = min(W, a.nh - kh0);
-  const auto rl = rev_last<N>(ax);
-  PointTile<W, C> tile{sm};
-  PointTile<W, C> &gst = tile;
-  // d = -1/((i2 + j2) + k2) with i2 = (min(i, ni-i)*ddi)^2 etc., as
-  // ParisPencil.cpp:276-279 forms it, times 1/N
-  const int ni = a.ni;
-  const double jd = double(min(j, a.nj - j)) * a.dd[1];
-  const double j2 = jd * jd;
-  const double ddi = a.dd[0], ddk = a.dd[2];
-  const double minvN = -a.invN;
-  auto filt = [&](int pos, int c, C v) -> C {
-    const int kx = rl(pos);
-    const int kh = kh0 + c;
-    if (c >= ncol) return v;
-    if ((kx | j | kh) == 0) return mk((T)0, (T)0);
-    const double id = double(min(kx, ni - kx)) * ddi;
-    const double kd = double(kh) * ddk;
-    const double d = recip_pos((id * id + j2) + kd * kd) * minvN;
-    return cscale(v, (T)d);
-  };
-  if constexpr (N > 0) {
-    constexpr int S = plan_stages(N);
-    constexpr int RF = plan_radix(N, S - 1);
-    if constexpr (S > 1) {
-      dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, TWX>(ax, tile, tile, tile, W);
-      fused_filter_stage<RF, W, NT, N, C>(N, tile, tile, filt);
-      __syncthreads();
-      dit_ct<N, S - 2, true, Map::ColFast, W, NT, TWX>(ax, tile, gst, W);
-    } else {
-      fused_filter_stage<RF, W, NT, N, C>(N, tile, gst, filt);
-    }
-  } else {
-    const int S = ax.nstages;
-    if (S > 1) dif_rt<false, Map::ColFast, W, NT, false>(ax, S - 1, tile, tile, tile, W);
-    with_radix(ax.radix[S - 1], [&](auto tag) {
-      constexpr int R = decltype(tag)::value;
-      if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, tile, gst, filt);
-      else fused_filter_stage<R, W, NT, 0, C>(n, tile, tile, filt);
-    });
-    __syncthreads();
-    if (S > 1) dit_rt<true, Map::ColFast, W, NT>(ax, S - 2, tile, gst, W);
-  }
-  fence_proxy_async_smem();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < n / box_rows; q++) tma_store_3d(tmap, 2 * W * kt, j, q * box_rows, sm + q * box_rows * W);
-    bulk_commit();
-    bulk_wait_read();
-  }
-}
-
-// Loads one strided tile with TMA into sm (boxes of box_rows rows) and waits
-// on mb for phase `parity` with an iteration limit.  Returns false on every
-// thread if the copy did not complete (the plan status word is set).  The
-// caller's earlier shared-memory accesses of sm must be fenced
-// (fence_proxy_async_smem) and barriered before the call.
-template <typename C, int W, bool XPASS>
-__device__ __forceinline__ bool tma_tile(const CUtensorMap *tmap, C *sm, uint64_t *mb, uint32_t parity, int n,
-                                         int box_rows, int o, int kt, int *status) {
-  if (threadIdx.x == 0) {
-    mbar_expect_tx(mb, (uint32_t)(n * W * sizeof(C)));
-    for (int q = 0; q < n / box_rows; q++) {
-      if (XPASS) tma_load_3d(sm + q * box_rows * W, tmap, 2 * W * kt, o, q * box_rows, mb);
-      else tma_load_3d(sm + q * box_rows * W, tmap, 2 * W * kt, q * box_rows, o, mb);
-    }
-  }
-  const bool ok = mbar_wait_bounded(mb, parity);
-  if (__syncthreads_or(!ok)) {
-    // report, and give the copy in flight a bounded chance to land before the
-    // block's shared memory is released
-    if (threadIdx.x == 0) {
-      atomicExch(status, kDevTmaTimeout);
-      mbar_wait_bounded(mb, parity);
-    }
-    return false;
-  }
-  return true;
-}
-
 // ------------------------------------------------- unfused pass kernels
 // (one launch per pass; used when the fused passes are switched off)
 // For specialised lengths (line blocks always 16-byte aligned, at least two
@@ -832,23 +713,28 @@ static EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// Tensor map of a half spectrum at `base` viewed as (2*nh reals, nj, ni) with
-// row pitch nhp complex values; box = one tile chunk of the y or x pass.
-template <typename T> static int spectrum_map(const ff_plan *p, void *base, const StridedCfg &cfg, bool xpass,
-                                              CUtensorMap *map) {
+// Tensor map of a half spectrum at `base` (ni planes of nj rows of nh complex
+// values, row pitch nhp) viewed as (2*nh reals, nj, ni); box = W columns by
+// box_rows rows of one plane (y pass) or box_rows planes of one row (x pass).
+int encode_spectrum_map(void *base, int ni, int nj, int nh, int nhp, size_t esz, int W, int box_rows, bool xpass,
+                        CUtensorMap *map) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) return set_error(FF_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  const cuuint64_t csz = 2 * sizeof(T);
-  cuuint64_t dims[3] = {(cuuint64_t)2 * p->nh, (cuuint64_t)p->n[1], (cuuint64_t)p->n[0]};
-  cuuint64_t strides[2] = {(cuuint64_t)p->nhp * csz, (cuuint64_t)p->nhp * csz * p->n[1]};
-  cuuint32_t box[3] = {(cuuint32_t)(2 * cfg.W), xpass ? 1u : (cuuint32_t)cfg.box_rows,
-                       xpass ? (cuuint32_t)cfg.box_rows : 1u};
+  const cuuint64_t csz = 2 * esz;
+  cuuint64_t dims[3] = {(cuuint64_t)2 * nh, (cuuint64_t)nj, (cuuint64_t)ni};
+  cuuint64_t strides[2] = {(cuuint64_t)nhp * csz, (cuuint64_t)nhp * csz * nj};
+  cuuint32_t box[3] = {(cuuint32_t)(2 * W), xpass ? 1u : (cuuint32_t)box_rows, xpass ? (cuuint32_t)box_rows : 1u};
   cuuint32_t estr[3] = {1, 1, 1};
-  const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const CUtensorMapDataType dt = esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   CUresult r = enc(map, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_error(FF_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return FF_OK;
+}
+
+template <typename T> static int spectrum_map(const ff_plan *p, void *base, const StridedCfg &cfg, bool xpass,
+                                              CUtensorMap *map) {
+  return encode_spectrum_map(base, p->n[0], p->n[1], p->nh, p->nhp, sizeof(T), cfg.W, cfg.box_rows, xpass, map);
 }
 
 template <typename T> static PassArgs<T> pass_args(const ff_plan *p) {

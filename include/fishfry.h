@@ -139,8 +139,10 @@ int ff_batch_solve(ff_batch *batch, void *const *density, void *const *potential
 int ff_batch_tune(ff_batch *batch, void *const *density, void *const *potential, void *stream, int reps);
 
 /* The tile shape pass `kind` (0..4) of grid `index` uses: W (line pairs for
- * the z passes, columns for the strided ones) and ct (1: compile-time plan). */
-int ff_batch_shape(const ff_batch *batch, int index, int kind, int *W, int *ct);
+ * the z passes, columns for the strided ones), ct (1: compile-time plan) and
+ * tma (1: one-plane tiles loaded by TMA boxes; 0: tiles of the flattened
+ * column index read straight from HBM).  Any pointer may be NULL. */
+int ff_batch_shape(const ff_batch *batch, int index, int kind, int *W, int *ct, int *tma);
 
 /* As ff_plan_check, for the batch's device status word. */
 int ff_batch_check(ff_batch *batch, void *stream);
@@ -191,6 +193,15 @@ int ff_server_submit(ff_server *server, const int n[3], int precision, const voi
 /* Waits up to timeout_ms (< 0: without limit) for the request; FF_OK when
  * its result is ready, FF_ERR_TIMEOUT otherwise.  info may be NULL. */
 int ff_server_wait(ff_server *server, uint64_t id, double timeout_ms, ff_request_info *info);
+
+/* Completion queue: the id (and timings) of the next request that finished
+ * and has not been returned by this call before, waiting up to timeout_ms
+ * (< 0: without limit); FF_ERR_TIMEOUT if none.  A finished request keeps
+ * its buffers until fetched or released, so a client that waits for
+ * requests in submission order can hold the budget with finished work while
+ * an earlier, larger request waits for memory; taking completions from this
+ * queue avoids that. */
+int ff_server_next(ff_server *server, double timeout_ms, uint64_t *id, ff_request_info *info);
 
 /* Copies a finished request's potential (ni*nj*nk values) to phi (host or
  * device; phi NULL copies nothing) and releases the request's buffers. */

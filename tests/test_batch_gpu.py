@@ -113,8 +113,8 @@ def test_batch_tuned_shapes_keep_parity(torch_cuda, ff, oracle, precision, tol):
     csz = 16 if precision == 0 else 8
     for g in range(len(batch)):
         for kind in range(5):
-            W, ct = batch.shape(g, kind)
-            assert W >= 1 and ct in (0, 1)
+            W, ct, tma = batch.shape(g, kind)
+            assert W >= 1 and ct in (0, 1) and tma in (0, 1)
             if kind in (1, 2, 3):
                 assert (W * csz) % 128 == 0
     fs = init_all(ff, batch, d, modes_for(ff), precision)
@@ -141,3 +141,20 @@ def test_batch_of_256_seeded_grids(torch_cuda, ff, oracle):
     for g in range(256):
         norms = ff.rel_norms(dims[g], p[g], modes_for(ff, 99)(dims[g]), 0)
         assert max(norms) < 1e-6, (g, dims[g], norms)
+
+
+def test_batch_tma_tiles_for_long_lines(torch_cuda, ff, oracle):
+    """Grids whose y or x lines have 256+ points and planes of 32+ columns use
+    one-plane TMA tiles by default (compile-time 256/512 and runtime 300/270
+    lengths)."""
+    # lengths the tuning test above does not tune for these passes (tuned
+    # shapes are remembered process-wide and would replace the defaults)
+    dims = [(512, 64, 80), (64, 256, 72), (300, 270, 64), (320, 8, 100)]
+    batch = ff.Batch(dims)
+    assert batch.shape(0, 2) == (8, 1, 1) and batch.shape(1, 1) == (8, 1, 1) and batch.shape(1, 3) == (8, 1, 1)
+    assert batch.shape(2, 2) == (8, 0, 1) and batch.shape(2, 1) == (8, 0, 1) and batch.shape(3, 2) == (8, 0, 1)
+    d, p = make_buffers(torch_cuda, batch, 0)
+    fs = init_all(ff, batch, d, modes_for(ff, 17), 0)
+    batch.solve(d, p)
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL, (g, dims[g])

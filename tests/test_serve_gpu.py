@@ -143,3 +143,38 @@ def test_server_wait_timeout_and_release(torch_cuda, ff):
             srv.wait(rid, timeout_ms=1)
     finally:
         srv.close()
+
+
+def test_server_completion_queue_under_a_full_budget(torch_cuda, ff):
+    """Requests taken in completion order (ff_server_next) and released at
+    once: a budget that holds a few requests drains a queue of mixed sizes
+    where waiting in submission order could hold memory with finished work."""
+    sizes = [(128, 128, 128), (32, 32, 32), (64, 48, 40), (96, 96, 96), (40, 36, 45)] * 6
+    budget = 2 * 2 * (128 * 128 * 65 * 16) + (1 << 20)
+    srv = ff.Server(budget, max_active=16)
+    try:
+        fields = {n: field(torch_cuda, ff, n, 0, 9) for n in set(sizes)}
+        ids = {srv.submit(n, fields[n], 0) for n in sizes}
+        got = set()
+        while len(got) < len(ids):
+            rid, lat, queue, run = srv.next(timeout_ms=30000)
+            assert rid in ids and rid not in got and lat >= run >= 0
+            got.add(rid)
+            srv.release(rid)
+        st = srv.stats()
+        assert st["completed"] == len(sizes) and st["peak_bytes"] <= budget
+    finally:
+        srv.close()
+
+
+def test_server_large_requests_use_tma_tiles_and_match_oracle(torch_cuda, ff, oracle):
+    """Lines of 256+ points on planes of many columns take the one-plane TMA
+    tiles in the strided passes."""
+    srv = ff.Server(1 << 31, max_active=8)
+    try:
+        for n, prec, tol in [((256, 64, 80), 0, FP64_TOL), ((40, 300, 160), 1, FP32_TOL),
+                             ((270, 256, 90), 0, FP64_TOL)]:
+            f, phi = solve_one(torch_cuda, ff, srv, n, prec, 21)
+            assert rel_l2(phi, oracle.solve(f)) <= tol, n
+    finally:
+        srv.close()
