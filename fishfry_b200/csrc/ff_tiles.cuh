@@ -100,6 +100,11 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
   using C = typename Cplx<T>::type;
   const int nk = N > 0 ? N : a.nk;
   const int nh = a.nh;
+  // split/extension loops walk k over nh rounded up to whole 128-byte rows,
+  // so each group of lanes that shares a shared-memory wavefront stays in one
+  // row (nh = n/2 + 1 is odd; a plain k = it % nh mapping straddles rows)
+  constexpr int RA = 128 / (int)sizeof(typename Cplx<T>::type);
+  const int nha = N > 0 ? (N / 2 + 1 + RA - 1) / RA * RA : (nh + RA - 1) / RA * RA;
   const int Asz = max(W * P, 2 * W * a.nhp);
   C *A = sm;
   C *B = A + ((Asz * (int)sizeof(C) + 127) & ~127) / (int)sizeof(C);
@@ -117,9 +122,10 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
     dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ld0, tA, tBrev, W);
     // split into the staging rows [line][kh] (pitch nhp) in A, then one copy out
     const T h = (T)0.5;
-    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-      const int k = it % nh;
-      const int c = it / nh;
+    for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+      const int k = it % nha;
+      const int c = it / nha;
+      if (k >= nh) continue;
       const C z = tB(k, c);
       const C w = tB(k == 0 ? 0 : nk - k, c);
       A[(2 * c) * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
@@ -141,9 +147,10 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
     const T h = (T)0.5;
     if constexpr (TMA_OUT) {
       // staged rows [line][kh] (pitch nhp) in A, then one copy out
-      for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-        const int k = it % nh;
-        const int c = it / nh;
+      for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+        const int k = it % nha;
+        const int c = it / nha;
+        if (k >= nh) continue;
         const C z = tB(k, c);
         const C w = tB(k == 0 ? 0 : nk - k, c);
         A[(2 * c) * a.nhp + k] = mk(h * (z.x + w.x), h * (z.y - w.y));
@@ -153,9 +160,10 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
       __syncthreads();
       bulk_out(spec + line0 * a.nhp, A, (size_t)nl * a.nhp);
     } else {
-      for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-        const int k = it % nh;
-        const int c = it / nh;
+      for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+        const int k = it % nha;
+        const int c = it / nha;
+        if (k >= nh) continue;
         const long la = line0 + 2 * c;
         if (la >= lend) continue;
         const C z = tB(k, c);
@@ -179,6 +187,11 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
   using C = typename Cplx<T>::type;
   const int nk = N > 0 ? N : a.nk;
   const int nh = a.nh;
+  // split/extension loops walk k over nh rounded up to whole 128-byte rows,
+  // so each group of lanes that shares a shared-memory wavefront stays in one
+  // row (nh = n/2 + 1 is odd; a plain k = it % nh mapping straddles rows)
+  constexpr int RA = 128 / (int)sizeof(typename Cplx<T>::type);
+  const int nha = N > 0 ? (N / 2 + 1 + RA - 1) / RA * RA : (nh + RA - 1) / RA * RA;
   const int Asz = max(W * P, 2 * W * a.nhp);
   C *A = sm;
   C *B = A + ((Asz * (int)sizeof(C) + 127) & ~127) / (int)sizeof(C);
@@ -196,9 +209,10 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
   };
   if constexpr (TMAIO) {
     if (!bulk_in(A, spec + line0 * a.nhp, (size_t)nl * a.nhp * sizeof(C), io)) return false;
-    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-      const int k = it % nh;
-      const int c = it / nh;
+    for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+      const int k = it % nha;
+      const int c = it / nha;
+      if (k >= nh) continue;
       const int la = 2 * c;
       const C sa = la < nl ? A[la * a.nhp + k] : mk((T)0, (T)0);
       const C sb = la + 1 < nl ? A[(la + 1) * a.nhp + k] : mk((T)0, (T)0);
@@ -220,9 +234,10 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
     bulk_out(out + line0 * nk, raw, (size_t)nl * nk);
     return true;
   } else {
-    for (int it = threadIdx.x; it < W * nh; it += kZThreads) {
-      const int k = it % nh;
-      const int c = it / nh;
+    for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+      const int k = it % nha;
+      const int c = it / nha;
+      if (k >= nh) continue;
       const long la = line0 + 2 * c;
       C sa = mk((T)0, (T)0), sb = mk((T)0, (T)0);
       if (la < lend) sa = __ldcg(spec + la * a.nhp + k);
