@@ -169,7 +169,11 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
       if (sh.ct) {
         switch (a.nk) {
 #define FF_CASE(NN) \
-  case NN: return z_fwd_tile<T, NN, false, true>(g.density, spec, a, zW, P, line0, nlines, sm, io);
+  case NN: {                                                                              \
+    const bool ok = z_fwd_tile<T, NN, true>(g.density, spec, a, zW, P, line0, nlines, sm, io);  \
+    parity ^= 1u;                                                                         \
+    return ok;                                                                            \
+  }
           FF_FOR_EACH_BATCH_N(FF_CASE)
 #undef FF_CASE
           default: break;
@@ -264,8 +268,9 @@ __global__ void __launch_bounds__(kZThreads, (KIND == 0 || KIND == 4) ? FF_BATCH
     }
     const int g = wl.entry[lo].x;
     if constexpr (KIND == 0) {
-      // the forward z pass reads its lines with thread loads: hint the lines
-      // of the tile claimed about one round later (ticket t + gridDim.x) into L2
+      // forward z pass: hint the lines of the tile claimed about one round
+      // later (ticket t + gridDim.x) into L2, where its inbound copy (bulk
+      // copy or thread loads) will find them
       const int t2 = t + (int)gridDim.x;
       if (threadIdx.x == 0 && t2 < total) {
         int a2 = lo, b2 = wl.nentry - 1;

@@ -40,9 +40,8 @@ namespace ff {
 // ------------------------------------------------- unfused pass kernels
 // (one launch per pass; used when the fused passes are switched off)
 // For specialised lengths (line blocks always 16-byte aligned, at least two
-// stages) the forward z pass reads its lines from the threads (coalesced) and
-// writes its spectrum rows with one bulk copy, and the inverse moves its line
-// blocks both ways with bulk copies; other lengths use the threads for both.
+// stages) both z passes move their line blocks both ways with bulk copies;
+// other lengths use the threads for both.
 template <typename T, int N>
 __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, typename Cplx<T>::type *spec,
                                                        const PassArgs<T> a, int W, int P) {
@@ -61,7 +60,7 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, 
       l2_prefetch(f + fl * a.nk, (uint32_t)(min((long)(2 * W), nlines - fl) * a.nk * sizeof(T)));
   }
   const ZTileIO io{&mbar, 0, a.status};
-  z_fwd_tile<T, N, false, (N > 0)>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+  z_fwd_tile<T, N, (N > 0), (N > 0)>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                             reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
 
@@ -682,10 +681,10 @@ template <typename T> static int configure(ff_plan *p) {
     fc.lag = std::min(ni, std::max(2, (3 * fc.grid + 2 * per_plane - 1) / (2 * per_plane)));
   }
   // The forward z pass runs one tile per block, three blocks per SM, each
-  // waiting on its thread-issued line loads.  Block b hints block
-  // b + l2_ahead's lines into L2, so that read is under way while the
-  // resident blocks compute and lands as L2 hits.  (The same hint slows the
-  // TMA-fed passes.)
+  // waiting for its inbound line block.  Block b hints block b + l2_ahead's
+  // lines into L2, so that read is under way while the resident blocks
+  // compute and the later bulk copy finds them in L2.  (The same hint on the
+  // strided passes' tensor tiles slowed them.)
   const char *ahead = getenv("FF_L2_AHEAD");
   p->l2_ahead = ahead ? std::max(0, atoi(ahead)) : 3 * p->num_sms;
   const char *mode = getenv("FF_PASSES");

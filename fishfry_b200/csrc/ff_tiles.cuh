@@ -43,9 +43,12 @@ template <int N, typename C> __device__ __forceinline__ typename RevLastOf<N>::t
 //
 // With TMAIO the tile's lines enter and leave by bulk copies between HBM and
 // shared memory (the copy engine moves them; the threads only touch shared
-// memory), using the buffers as staging: the real lines land in B, the stages
-// run in A, the last stage writes B, and the output is staged in A.  Without
-// TMAIO the first stage reads HBM and the output is written from registers.
+// memory), using the buffers as staging.  Forward: the real lines land in B,
+// the stages run in A, the last stage writes B, and the output is staged in A.
+// Inverse: the spectrum rows land in A, the first stage reads them, the
+// stages run in B, the last writes A, and the output lines are staged in B.
+// Without TMAIO the first stage reads HBM and the output is written from
+// registers.
 // A holds max(W*P, 2W*nhp) complex values, B holds W*P (+ 128 bytes slack).
 struct ZTileIO {
   uint64_t *mbar;      // TMAIO: barrier of the inbound copy
@@ -209,23 +212,29 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
   };
   if constexpr (TMAIO) {
     if (!bulk_in(A, spec + line0 * a.nhp, (size_t)nl * a.nhp * sizeof(C), io)) return false;
-    for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
-      const int k = it % nha;
-      const int c = it / nha;
-      if (k >= nh) continue;
+    // The first stage reads Z straight from the spectrum rows in A, forming
+    // the Hermitian extension on the fly (the same values hermitian() writes:
+    // Z[k] = A[k] + i B[k] for k <= nk/2, conj A[nk-k] + i conj B[nk-k] above,
+    // imaginary parts dropped at k = 0 and nk/2), and writes B; the stages
+    // run in B and the last writes natural order into A, whose rows are no
+    // longer needed after the first stage.
+    auto ldh = [&](int pos, int c) -> C {
       const int la = 2 * c;
+      const bool lo = 2 * pos <= nk;
+      const int k = lo ? pos : nk - pos;
       const C sa = la < nl ? A[la * a.nhp + k] : mk((T)0, (T)0);
       const C sb = la + 1 < nl ? A[(la + 1) * a.nhp + k] : mk((T)0, (T)0);
-      hermitian(k, c, sa, sb);
-    }
-    __syncthreads();
-    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, tB, tA, tBrev, W);
-    // real lines staged in A, then one copy out
-    T *raw = reinterpret_cast<T *>(A);
+      if (k == 0 || 2 * k == nk) return mk(sa.x, sb.x);
+      return lo ? mk(sa.x - sb.y, sa.y + sb.x) : mk(sa.x + sb.y, sb.x - sa.y);
+    };
+    LineTileRev<C, typename RevLastOf<N>::type> tArev{tA, rev_last<N>(ax)};
+    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, ldh, tB, tArev, W);
+    // real lines staged in B, then one copy out
+    T *raw = reinterpret_cast<T *>(B);
     for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
       const int t = it % nk;
       const int c = it / nk;
-      const C v = tB(t, c);
+      const C v = tA(t, c);
       raw[(2 * c) * nk + t] = v.x;
       raw[(2 * c + 1) * nk + t] = v.y;
     }
