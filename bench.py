@@ -62,6 +62,7 @@ def parse():
                     help="serve: arrival rates (requests/s)")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM admission budget")
     ap.add_argument("--seed", type=int, default=12345)
+    ap.add_argument("--no-tune", action="store_true", help="batch: default tile shapes, no autotuning")
     return ap.parse_args()
 
 
@@ -506,7 +507,8 @@ def run_batch(args):
         b = ff.Batch(dims, precision=prec)
         d = [torch.empty(nb // esz, dtype=dt, device=dev) for nb in b.nbytes]
         p = [torch.empty(nb // esz, dtype=dt, device=dev) for nb in b.nbytes]
-        b.tune(d, p, stream=stream, reps=3)
+        if not args.no_tune:
+            b.tune(d, p, stream=stream, reps=3)
         f0 = []
         for g, n in enumerate(dims):
             x = torch.empty(n[0] * n[1] * n[2], dtype=dt, device=dev)
@@ -563,7 +565,8 @@ def run_batch(args):
         "value": out[ff.FF_FP32]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": W,
         "ms_per_step": out[ff.FF_FP32]["ms"], "higher_is_better": True, "dtype": "f32",
         "data": "synthetic: analytic f + 64 seeded modes per grid", "config": {
-            "workload": "256 grids, dims seed 2024, five persistent launches per solve (CUDA graph), tuned tiles",
+            "workload": "256 grids, dims seed 2024, five persistent launches per solve (CUDA graph), %s tiles" % (
+                "default" if args.no_tune else "tuned"),
             "points_per_batch": pts},
         "fp32_batch": {k: v for k, v in out[ff.FF_FP32].items() if k != "phi"},
         "fp64_batch": {k: v for k, v in out[ff.FF_FP64].items() if k != "phi"},
