@@ -220,6 +220,27 @@ def reference_sample_grid(n, steps, budget_s=150.0):
     return (64, 64, 64)
 
 
+def scipy_yardstick(n, threads):
+    """A library yardstick on the host cores: the same spectral solve with
+    scipy.fft (pocketfft) rfftn/irfftn on all threads, one timed solve of the
+    FP64 analytic f (seconds, points/s)."""
+    import numpy as np
+    import scipy.fft as sf
+    from oracle import oracle as O
+    f = O.init_f(tuple(n))
+    kx = [np.minimum(np.arange(m), m - np.arange(m)).astype(np.float64) for m in n[:2]]
+    kz = np.arange(n[2] // 2 + 1, dtype=np.float64)
+    k2 = kx[0][:, None, None] ** 2 + kx[1][None, :, None] ** 2 + kz[None, None, :] ** 2
+    k2[0, 0, 0] = np.inf
+    t = time.perf_counter()
+    s = sf.rfftn(f, workers=threads)
+    s *= -1.0 / k2
+    phi = sf.irfftn(s, s=f.shape, workers=threads)
+    dt = time.perf_counter() - t
+    del phi
+    return dt, f.size / dt
+
+
 def run_reference(args):
     """The reference's algorithm on the host cores: each step one oracle
     solve (ParisPencil's FFT solve restated in C++/OpenMP) of a sample grid
@@ -246,6 +267,23 @@ def run_reference(args):
         "note": "the reference has no CPU code path; this is the oracle's OpenMP restatement of its algorithm",
     }
     print(json.dumps(line), flush=True)
+
+
+def job_time_ms(local_ms, world, device):
+    """The job's time: the max over ranks of each rank's timed region (every
+    rank receives it).  One rank per GPU; on the CPU (gloo) for tests."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(points_per_rank, steps, job_ms, world):
+    """Whole-job points/s of N replicas (weak scaling: every rank solves its
+    own grid of points_per_rank points per step)."""
+    return world * points_per_rank * steps / (job_ms * 1e-3)
 
 
 def run_ours(args):
@@ -301,12 +339,9 @@ def run_ours(args):
     total_ms = sum(t for _, t in rec)
     nph = plan.phases()
     pass_ms = [sum(r[0][q] for r in rec) / len(rec) for q in range(nph)]
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = job_time_ms(total_ms, world, dev)
     ms_per_step = total_ms / args.steps
-    value = world * N * args.steps / (total_ms * 1e-3)
+    value = replicas_value(N, args.steps, total_ms, world)
 
     # correctness of the last solve (outside timing)
     norms = ff.rel_norms(n, p, None, prec)
@@ -360,12 +395,9 @@ def run_ours(args):
         s_out.wait_event(last)
         e1.record(s_out)
         e1.synchronize()
-        te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_ms = float(te.item())
+        e2e_ms = job_time_ms(e0.elapsed_time(e1), world, dev)
         same = bool(torch.equal(hp[(args.steps - 1) % 2].to(dev), ref))
-        e2e = {"value": world * N * args.steps / (e2e_ms * 1e-3), "unit": "points/s",
+        e2e = {"value": replicas_value(N, args.steps, e2e_ms, world), "unit": "points/s",
                "h2d_bytes_per_step": N * esz, "d2h_bytes_per_step": N * esz,
                "ms_per_step": e2e_ms / args.steps, "pipelined": "two buffer sets, copies on their own streams",
                "result_matches_device_timed_solve": same}
@@ -391,6 +423,12 @@ def run_ours(args):
             times, cores = oracle_baseline(n, steps=1, warmup=0)
             cpu = {"value": N / times[0], "unit": "points/s", "cores": cores, "kind": "port",
                    "sample": "one full %dx%dx%d FP64 solve of the oracle (OpenMP) on %s" % (*n, cpu_info() or "host")}
+            try:
+                sec, pps = scipy_yardstick(n, cores)
+                cpu["scipy_fft_yardstick"] = {"value": pps, "unit": "points/s", "seconds": sec, "workers": cores,
+                                              "what": "scipy.fft rfftn, -1/k^2, irfftn (pocketfft), one solve"}
+            except Exception as e:   # a missing scipy does not cost the line
+                cpu["scipy_fft_yardstick"] = {"unavailable": str(e)[:120]}
         line = {
             "metric": "512^3 FP64 solve points/s", "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
