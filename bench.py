@@ -715,6 +715,37 @@ def run_serve(args):
                         "points_per_s": st["points_per_s"], "completed": st["completed"],
                         "peak_gb": st["peak_bytes"] / 1e9, "steps": st["steps"], "launches": st["launches"],
                         "max_active": st["max_active"]})
+    # the plain method on the same mix: single-grid solves one after another
+    # (plans made beforehand, each request's field copied in first, as the
+    # server copies it), FP64 and FP32, on a sample of the request stream
+    rng = np.random.default_rng(args.seed + 7)
+    sample = [serve_dims(rng) for _ in range(min(400, args.requests))]
+    plain = {}
+    for prec in (ff.FF_FP64, ff.FF_FP32):
+        dt = torch.float64 if prec == ff.FF_FP64 else torch.float32
+        plans = {n: ff.Plan(n, precision=prec) for n in set(sample)}
+        cap = max(pl.nbytes for pl in plans.values())
+        esz = 8 if prec == ff.FF_FP64 else 4
+        d = torch.empty(cap // esz, dtype=dt, device=dev)
+        p = torch.empty_like(d)
+        st = torch.cuda.Stream(device=dev)
+        for rep in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for n in sample:
+                N = n[0] * n[1] * n[2]
+                with torch.cuda.stream(st):
+                    d[:N].copy_(src[prec][:N])
+                plans[n].solve(d, p, stream=st, nbytes=cap)
+            e1.record(st)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        plain["fp64" if prec == ff.FF_FP64 else "fp32"] = {"solves_per_s": len(sample) / (ms * 1e-3),
+                                                           "requests": len(sample)}
+        for pl in plans.values():
+            pl.close()
+        del d, p
+        torch.cuda.empty_cache()
     # accuracy sample: FP32 requests against the plain FP64 solve of the same f
     srv = ff.Server(int(min(args.budget_gb, 40) * 1e9), max_active=64)
     rng = np.random.default_rng(args.seed)
@@ -746,6 +777,8 @@ def run_serve(args):
         "config": {"workload": "continuous batching request loop", "requests_per_rate": args.requests,
                    "budget_gb": args.budget_gb, "seed": args.seed},
         "rates": results,
+        "plain_loop_on_the_same_mix": plain,
+        "served_at_saturation_vs_plain_fp64": max(r["solves_per_s"] for r in results) / plain["fp64"]["solves_per_s"],
         "fp32_vs_plain_fp64_rel_l2_max": worst,
     }
     print(json.dumps(line), flush=True)

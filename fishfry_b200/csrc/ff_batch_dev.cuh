@@ -94,14 +94,14 @@ __device__ __forceinline__ void cols_tile(const PassArgs<T> &a, const typename C
     } else {
       const int S = ax.nstages;
       const int n = ax.n;
-      if (S > 1) dif_rt<false, Map::ColFast, W, NT, false>(ax, S - 1, ld0, tl, tl, W);
+      if (S > 1) dif_rt<false, Map::ColFast, W, NT, false, TWR>(ax, S - 1, ld0, tl, tl, W);
       with_radix(ax.radix[S - 1], [&](auto tag) {
         constexpr int R = decltype(tag)::value;
         if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, ld0, gst, filt);
         else fused_filter_stage<R, W, NT, 0, C>(n, tl, tl, filt);
       });
       __syncthreads();
-      if (S > 1) dit_rt<true, Map::ColFast, W, NT>(ax, S - 2, tl, gst, W);
+      if (S > 1) dit_rt<true, Map::ColFast, W, NT, TWR>(ax, S - 2, tl, gst, W);
     }
   }
 }

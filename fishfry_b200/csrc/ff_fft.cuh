@@ -269,12 +269,16 @@ __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, 
     const int j = b - blk * m;
     const int base = blk * L + j;
     C v[R];
-    // Compile-time stage with twiddles: the factors are fetched before the
-    // data loads and applied without a branch (j = 0 reads exp(0) = 1), so
-    // their latency overlaps the data loads.  Not for FP64 line-major tiles,
-    // where the extra live registers spill.
+    // Stage with twiddles: the factors are fetched before the data loads and
+    // applied without a branch (j = 0 reads exp(0) = 1), so their latency
+    // overlaps the data loads.  Not for FP64 line-major tiles, where the
+    // extra live registers spill.
     constexpr bool kPrefetch = !(MAP == Map::PosFast && sizeof(C) == 16);
-    if constexpr (NC > 0 && LC > R && R > 1 && kPrefetch) {
+    // runtime plans take the same path in every stage that has twiddles
+    // (span above the radix); the branch is uniform across the block
+    bool pf = false;
+    if constexpr (R > 1 && kPrefetch) pf = NC > 0 ? (LC > R) : (L > R);
+    if constexpr (R > 1 && kPrefetch) if (pf) {
       if constexpr (TWREC) {
         double2 w1 = __ldg(ax.tw64 + j * twstep);
 #pragma unroll
@@ -305,7 +309,9 @@ __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, 
       }
 #pragma unroll
       for (int r = 0; r < R; r++) st(base + r * m, c, v[r]);
-    } else {
+      return;
+    }
+    {
 #pragma unroll
       for (int r = 0; r < R; r++) v[r] = ld(base + r * m, c);
       if (DIT) {
@@ -413,16 +419,17 @@ template <typename C, typename RL> struct LineTileRev {
 // Runtime plan.  DIF stages 0..S-1: stage 0 reads ld0 (with recurrence
 // twiddles if TWREC0), stage S-1 writes stl, the others read and write mid.
 // A block barrier follows every stage.
-template <bool INV, Map MAP, int W, int NT, bool TWREC0, typename C, typename LD0, typename MID, typename STL>
+template <bool INV, Map MAP, int W, int NT, bool TWREC0, bool TWALL = false, typename C, typename LD0, typename MID,
+          typename STL>
 __device__ __forceinline__ void dif_rt(const AxisDev<C> &ax, int S, LD0 &ld0, MID &mid, STL &stl, int ncols) {
   int L = ax.n;
   for (int s = 0; s < S; s++) {
     with_radix(ax.radix[s], [&](auto tag) {
       constexpr int R = decltype(tag)::value;
-      if (s == 0 && s == S - 1) stage<R, INV, false, MAP, W, NT, 0, 0, TWREC0>(ax.n, L, ax, ld0, stl, ncols);
-      else if (s == 0) stage<R, INV, false, MAP, W, NT, 0, 0, TWREC0>(ax.n, L, ax, ld0, mid, ncols);
-      else if (s == S - 1) stage<R, INV, false, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, stl, ncols);
-      else stage<R, INV, false, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, mid, ncols);
+      if (s == 0 && s == S - 1) stage<R, INV, false, MAP, W, NT, 0, 0, TWREC0 || TWALL>(ax.n, L, ax, ld0, stl, ncols);
+      else if (s == 0) stage<R, INV, false, MAP, W, NT, 0, 0, TWREC0 || TWALL>(ax.n, L, ax, ld0, mid, ncols);
+      else if (s == S - 1) stage<R, INV, false, MAP, W, NT, 0, 0, TWALL>(ax.n, L, ax, mid, stl, ncols);
+      else stage<R, INV, false, MAP, W, NT, 0, 0, TWALL>(ax.n, L, ax, mid, mid, ncols);
     });
     L /= ax.radix[s];
     __syncthreads();
@@ -431,15 +438,15 @@ __device__ __forceinline__ void dif_rt(const AxisDev<C> &ax, int S, LD0 &ld0, MI
 
 // Runtime plan.  DIT stages s_begin..0 on a digit-reversed tile in mid;
 // stage 0 writes stl.  A block barrier follows every stage.
-template <bool INV, Map MAP, int W, int NT, typename C, typename MID, typename STL>
+template <bool INV, Map MAP, int W, int NT, bool TWALL = false, typename C, typename MID, typename STL>
 __device__ __forceinline__ void dit_rt(const AxisDev<C> &ax, int s_begin, MID &mid, STL &stl, int ncols) {
   for (int s = s_begin; s >= 0; s--) {
     int L = ax.n;
     for (int q = 0; q < s; q++) L /= ax.radix[q];
     with_radix(ax.radix[s], [&](auto tag) {
       constexpr int R = decltype(tag)::value;
-      if (s == 0) stage<R, INV, true, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, stl, ncols);
-      else stage<R, INV, true, MAP, W, NT, 0, 0, false>(ax.n, L, ax, mid, mid, ncols);
+      if (s == 0) stage<R, INV, true, MAP, W, NT, 0, 0, TWALL>(ax.n, L, ax, mid, stl, ncols);
+      else stage<R, INV, true, MAP, W, NT, 0, 0, TWALL>(ax.n, L, ax, mid, mid, ncols);
     });
     __syncthreads();
   }
@@ -483,7 +490,7 @@ template <int N, bool INV, Map MAP, int W, int NT, bool TWREC0, bool TWALL, type
           typename STL>
 __device__ __forceinline__ void dif_all(const AxisDev<C> &ax, LD0 &ld0, MID &mid, STL &stl, int ncols) {
   if constexpr (N > 0) dif_ct<N, plan_stages(N), 0, INV, MAP, W, NT, TWREC0, TWALL>(ax, ld0, mid, stl, ncols);
-  else dif_rt<INV, MAP, W, NT, TWREC0>(ax, ax.nstages, ld0, mid, stl, ncols);
+  else dif_rt<INV, MAP, W, NT, TWREC0, TWALL>(ax, ax.nstages, ld0, mid, stl, ncols);
 }
 
 // ------------------------------------------------ TMA and mbarrier helpers

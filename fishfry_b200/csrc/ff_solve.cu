@@ -39,10 +39,12 @@ namespace ff {
 
 // ------------------------------------------------- unfused pass kernels
 // (one launch per pass; used when the fused passes are switched off)
-// For specialised lengths (line blocks always 16-byte aligned, at least two
-// stages) both z passes move their line blocks both ways with bulk copies;
-// other lengths use the threads for both.
-template <typename T, int N>
+// With BULK (every specialised length, and runtime lengths whose lines are
+// whole 16-byte multiples and whose plan has at least two stages) both z
+// passes move their line blocks both ways with bulk copies; otherwise the
+// threads load the lines, and the inverse stores them.  The spectrum rows
+// always leave (forward) and enter (inverse) as 16-byte multiples.
+template <typename T, int N, bool BULK>
 __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, typename Cplx<T>::type *spec,
                                                        const PassArgs<T> a, int W, int P) {
   extern __shared__ unsigned char smraw[];
@@ -53,18 +55,18 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, 
   }
   __syncthreads();
   const long nlines = (long)a.ni * a.nj;
-  if (N > 0 && threadIdx.x == 0) {
-    // whole lines of a specialised length are 16-byte multiples
+  if (BULK && threadIdx.x == 0) {
+    // whole lines are 16-byte multiples here
     const long fl = ((long)blockIdx.x + a.l2_ahead) * (2 * W);
     if (a.l2_ahead > 0 && fl < nlines)
       l2_prefetch(f + fl * a.nk, (uint32_t)(min((long)(2 * W), nlines - fl) * a.nk * sizeof(T)));
   }
   const ZTileIO io{&mbar, 0, a.status};
-  z_fwd_tile<T, N, (N > 0), (N > 0)>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
-                            reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
+  z_fwd_tile<T, N, BULK, true>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+                               reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
 
-template <typename T, int N>
+template <typename T, int N, bool BULK>
 __global__ void __launch_bounds__(kZThreads, 3) k_zinv(const typename Cplx<T>::type *spec, T *__restrict__ out,
                                                        const PassArgs<T> a, int W, int P) {
   extern __shared__ unsigned char smraw[];
@@ -76,8 +78,8 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zinv(const typename Cplx<T>::t
   __syncthreads();
   const long nlines = (long)a.ni * a.nj;
   const ZTileIO io{&mbar, 0, a.status};
-  z_inv_tile<T, N, (N > 0)>(spec, out, a, W, P, (long)blockIdx.x * (2 * W), nlines,
-                            reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
+  z_inv_tile<T, N, BULK>(spec, out, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+                         reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
 
 // One TMA-loaded strided tile per block (y forward / inverse or x).  Blocks
@@ -471,6 +473,7 @@ struct ff_plan {
   int *counters;       // fused passes: 2 tickets + 2 x ni plane counts
   int fused;           // 1: three launches (fused z/y passes), 0: five launches
   int zN;              // z passes: specialised length, 0 = runtime plan
+  bool zbulk;          // z passes: line blocks by bulk copies
   int zW, zP;          // z passes: line pairs per block, line pitch in complex values
   size_t zsmem;
   unsigned ztiles;
@@ -554,17 +557,18 @@ static int special_n(int n) {
   return 0;
 }
 
-template <typename T> static ZFwdKernel<T> zfwd_kernel(int N) {
-#define FF_CASE(NN) if (N == NN) return k_zfwd<T, NN>;
+// bulk: line blocks by bulk copies (always for specialised lengths)
+template <typename T> static ZFwdKernel<T> zfwd_kernel(int N, bool bulk) {
+#define FF_CASE(NN) if (N == NN) return k_zfwd<T, NN, true>;
   FF_FOR_EACH_SPECIAL_N(FF_CASE)
 #undef FF_CASE
-  return k_zfwd<T, 0>;
+  return bulk ? k_zfwd<T, 0, true> : k_zfwd<T, 0, false>;
 }
-template <typename T> static ZInvKernel<T> zinv_kernel(int N) {
-#define FF_CASE(NN) if (N == NN) return k_zinv<T, NN>;
+template <typename T> static ZInvKernel<T> zinv_kernel(int N, bool bulk) {
+#define FF_CASE(NN) if (N == NN) return k_zinv<T, NN, true>;
   FF_FOR_EACH_SPECIAL_N(FF_CASE)
 #undef FF_CASE
-  return k_zinv<T, 0>;
+  return bulk ? k_zinv<T, 0, true> : k_zinv<T, 0, false>;
 }
 
 // kind: 0 = y forward, 1 = y inverse, 2 = x (forward, filter, inverse);
@@ -629,8 +633,12 @@ template <typename T> static int configure(ff_plan *p) {
   p->zsmem = a_bytes + (size_t)p->zW * p->zP * csz + 128 + 128;
   const long npairs = ((long)ni * nj + 1) / 2;
   p->ztiles = (unsigned)((npairs + p->zW - 1) / p->zW);
-  int rc = allow_dyn_smem(zfwd_kernel<T>(p->zN), nullptr);
-  if (rc == FF_OK) rc = allow_dyn_smem(zinv_kernel<T>(p->zN), nullptr);
+  // line blocks by bulk copies: whole 16-byte multiples, and a first stage
+  // that is not the last (the bulk-fed tiles stage their input in the buffer
+  // the last stage writes)
+  p->zbulk = p->zN > 0 || ((nk * sizeof(T)) % 16 == 0 && plan_stages(nk) >= 2);
+  int rc = allow_dyn_smem(zfwd_kernel<T>(p->zN, p->zbulk), nullptr);
+  if (rc == FF_OK) rc = allow_dyn_smem(zinv_kernel<T>(p->zN, p->zbulk), nullptr);
   if (rc != FF_OK) return rc;
   // strided tiles: W 128-byte columns x n rows, one per block
   const int W = 128 / (int)csz;
@@ -787,7 +795,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
     return FF_OK;
   }
-  zfwd_kernel<T>(p->zN)<<<p->ztiles, kZThreads, p->zsmem, st>>>(D, Ps, a, p->zW, p->zP);
+  zfwd_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(D, Ps, a, p->zW, p->zP);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
   strided_kernel<T>(0, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ps, a, p->ycfg.box_rows);
@@ -799,7 +807,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
   strided_kernel<T>(1, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ds, a, p->ycfg.box_rows);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
-  zinv_kernel<T>(p->zN)<<<p->ztiles, kZThreads, p->zsmem, st>>>(Ds, P, a, p->zW, p->zP);
+  zinv_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(Ds, P, a, p->zW, p->zP);
   FF_CUDA(cudaGetLastError());
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
   return FF_OK;

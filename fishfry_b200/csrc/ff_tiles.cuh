@@ -381,14 +381,14 @@ __device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T
     }
   } else {
     const int S = ax.nstages;
-    if (S > 1) dif_rt<false, Map::ColFast, W, NT, false>(ax, S - 1, tile, tile, tile, W);
+    if (S > 1) dif_rt<false, Map::ColFast, W, NT, false, TWX>(ax, S - 1, tile, tile, tile, W);
     with_radix(ax.radix[S - 1], [&](auto tag) {
       constexpr int R = decltype(tag)::value;
       if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, tile, gst, filt);
       else fused_filter_stage<R, W, NT, 0, C>(n, tile, tile, filt);
     });
     __syncthreads();
-    if (S > 1) dit_rt<true, Map::ColFast, W, NT>(ax, S - 2, tile, gst, W);
+    if (S > 1) dit_rt<true, Map::ColFast, W, NT, TWX>(ax, S - 2, tile, gst, W);
   }
   fence_proxy_async_smem();
   __syncthreads();
