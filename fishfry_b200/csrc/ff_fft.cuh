@@ -248,6 +248,25 @@ enum class Map { ColFast, PosFast };
 //   NT > 0: compile-time block size; with NC it fully unrolls the item loop.
 //   TWMUL: the twiddle table is TWMUL times longer than n (a sub-transform of
 //   a longer line uses that line's table).
+// Quotient and remainder by a divisor fixed for a whole stage, from its
+// correctly rounded FP32 reciprocal and one correction step: exact for
+// 0 <= x < 2^20 (the item indices of a tile), where the FP32 quotient is off
+// by less than one.  Compile-time divisors use plain division (the compiler
+// turns it into multiplies).
+struct StageDiv {
+  int d;
+  float inv;
+  __device__ __forceinline__ explicit StageDiv(int dd) : d(dd), inv(1.0f / (float)dd) {}
+  __device__ __forceinline__ int quot(int x, int &rem) const {
+    int q = __float2int_rz((float)x * inv);
+    int r = x - q * d;
+    if (r < 0) { q--; r += d; }
+    else if (r >= d) { q++; r -= d; }
+    rem = r;
+    return q;
+  }
+};
+
 template <int R, bool INV, bool DIT, Map MAP, int W, int NT, int NC, int LC, bool TWREC, int TWMUL = 1, typename C,
           typename LD, typename ST>
 __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, LD &ld, ST &st, int ncols) {
@@ -256,17 +275,28 @@ __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, 
   const int m = L / R;
   const int twstep = TWMUL * n / L;
   const int nb = n / R;
+  // runtime divisors by reciprocal, except on FP64 line-major tiles (their
+  // registers are the tightest; measured slower there)
+  constexpr bool kRcpDiv = NC == 0 && !(MAP == Map::PosFast && sizeof(C) == 16);
+  const StageDiv dm(kRcpDiv ? m : 1), dnb(kRcpDiv ? nb : 1);
   auto body = [&](int it) {
     int c, b;
     if (MAP == Map::ColFast) {
       c = it % W;
       b = it / W;
-    } else {
+    } else if (!kRcpDiv) {
       b = it % nb;
       c = it / nb;
+    } else {
+      c = dnb.quot(it, b);
     }
-    const int blk = b / m;
-    const int j = b - blk * m;
+    int blk, j;
+    if (!kRcpDiv) {
+      blk = b / m;
+      j = b - blk * m;
+    } else {
+      blk = dm.quot(b, j);
+    }
     const int base = blk * L + j;
     C v[R];
     // Stage with twiddles: the factors are fetched before the data loads and
