@@ -113,6 +113,13 @@ size_t batch_shape_smem(int precision, const BatchGridHost &g, int kind, const T
   return batch_tile_smem(kind, batch_axis_len(g, kind), g.n[2], g.nhp, s.W, precision == FF_FP64 ? 16 : 8);
 }
 
+// z passes of a runtime length may move line blocks by bulk copies when the
+// lines are 16-byte multiples and the plan has two or more stages (the tile
+// stages its input in the buffer the last stage writes).
+bool batch_z_bulk_ok(int precision, int nk) {
+  return ((size_t)nk * (precision == FF_FP64 ? 8 : 4)) % 16 == 0 && plan_stages(nk) >= 2;
+}
+
 bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const TileShape &s) {
   if (s.W < 1) return false;
   if (s.ct && !batch_special_n(batch_axis_len(g, kind))) return false;
@@ -120,7 +127,7 @@ bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const Ti
     const int w1 = 128 / (precision == FF_FP64 ? 16 : 8);
     if (s.W != w1 && s.W != 2 * w1 && s.W != 4 * w1) return false;
     if (s.tma && s.W != w1) return false;
-  } else if (s.tma) {
+  } else if (s.tma && !batch_z_bulk_ok(precision, g.n[2])) {
     return false;
   }
   return batch_shape_smem(precision, g, kind, s) <= kBatchSmem;
@@ -138,6 +145,9 @@ TileShape batch_default_shape(int precision, const BatchGridHost &g, int kind) {
     W = (int)std::min<long>(W, npairs);
     while (W > 1 && !batch_shape_valid(precision, g, kind, TileShape{W, s.ct, 0})) W--;
     s.W = W;
+    // runtime lengths: bulk-copied line blocks where the lines allow them
+    // (compile-time lengths always use them)
+    s.tma = !s.ct && batch_z_bulk_ok(precision, g.n[2]) ? 1 : 0;
     return s;
   }
   const int w1 = 128 / (precision == FF_FP64 ? 16 : 8);
@@ -571,7 +581,10 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
       const TileShape d = batch_default_shape(b->precision, ref, k);
       for (int ct = batch_special_n(n) ? 1 : 0; ct >= 0; ct--) {
         if (k == 0 || k == 4) {
-          for (int W : {std::max(1, d.W / 2), d.W, d.W * 2}) cand.push_back(TileShape{W, ct, 0});
+          for (int W : {std::max(1, d.W / 2), d.W, d.W * 2}) {
+            cand.push_back(TileShape{W, ct, 0});
+            if (!ct) cand.push_back(TileShape{W, 0, 1});
+          }
         } else {
           const int w1 = 128 / (int)b->csz;
           for (int m : {1, 2, 4}) cand.push_back(TileShape{m * w1, ct, 0});

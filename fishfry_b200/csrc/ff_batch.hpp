@@ -50,9 +50,11 @@ struct BatchWork {
 // strided passes take W columns (W * sizeof(complex) a multiple of 128
 // bytes: 1, 2 or 4 rows of 128 bytes).  ct = 1 selects the compile-time
 // specialised tile for the axis length (batch_special_n), 0 the runtime plan.
-// tma = 1 (strided passes only, W = 128 bytes of columns): the tile is W kh
+// Strided passes: tma = 1 (W = 128 bytes of columns) is a tile of W kh
 // columns of one plane, loaded by TMA boxes as in the single-grid passes;
-// tma = 0: W columns of the flattened (plane, kh) index, read straight from HBM.
+// tma = 0 is W columns of the flattened (plane, kh) index, read straight from
+// HBM.  z passes of runtime lengths: tma = 1 moves the line blocks by bulk
+// copies (compile-time lengths always do).
 struct TileShape {
   int W;
   int ct;
@@ -122,5 +124,6 @@ void batch_grid_init(BatchGridHost &h, const int n[3], const double *lo, const d
 size_t batch_grid_bytes(const BatchGridHost &h, int precision);
 // Axis checks of one grid (status and message as the C ABI reports them).
 int batch_check_dims(const int n[3], const double *lo, const double *hi, const char *who, int g);
+bool batch_z_bulk_ok(int precision, int nk);
 
 }  // namespace ff

@@ -179,6 +179,11 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
           default: break;
         }
       }
+      if (sh.tma) {
+        const bool ok = z_fwd_tile<T, 0, true>(g.density, spec, a, zW, P, line0, nlines, sm, io);
+        parity ^= 1u;
+        return ok;
+      }
       return z_fwd_tile<T, 0, false, false>(g.density, spec, a, zW, P, line0, nlines, sm, io);
     } else {
       const C *spec = reinterpret_cast<const C *>(g.density);
@@ -194,6 +199,11 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
 #undef FF_CASE
           default: break;
         }
+      }
+      if (sh.tma) {
+        const bool ok = z_inv_tile<T, 0, true>(spec, g.potential, a, zW, P, line0, nlines, sm, io);
+        parity ^= 1u;
+        return ok;
       }
       return z_inv_tile<T, 0, false>(spec, g.potential, a, zW, P, line0, nlines, sm, io);
     }

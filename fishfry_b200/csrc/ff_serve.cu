@@ -113,6 +113,11 @@ struct Lane {
   int precision = FF_FP64;
   size_t dsz = 0;
   cudaStream_t stream = nullptr;
+  // a step forks from `stream` into one stream per pass kind, so the kinds'
+  // launches (independent requests) overlap, and joins back before its event
+  cudaStream_t kstream[5] = {};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t kev[5] = {};
   void *desc = nullptr;                    // device descriptors [slots]
   unsigned char *desc_host = nullptr;      // pinned image
   CUtensorMap *maps = nullptr;             // device tensor maps [slots][2] (y, x boxes of the potential)
@@ -184,6 +189,11 @@ int lane_init(ff_server *s, Lane &L, int precision) {
   L.precision = precision;
   L.dsz = precision == FF_FP64 ? batch_desc_size<double>() : batch_desc_size<float>();
   FF_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+  FF_CUDA(cudaEventCreateWithFlags(&L.fork_ev, cudaEventDisableTiming));
+  for (int k = 0; k < 5; k++) {
+    FF_CUDA(cudaStreamCreateWithFlags(&L.kstream[k], cudaStreamNonBlocking));
+    FF_CUDA(cudaEventCreateWithFlags(&L.kev[k], cudaEventDisableTiming));
+  }
   FF_CUDA(cudaMalloc(&L.desc, slots * L.dsz));
   FF_CUDA(cudaMallocHost((void **)&L.desc_host, slots * L.dsz));
   FF_CUDA(cudaMalloc((void **)&L.maps, (size_t)slots * 2 * sizeof(CUtensorMap)));
@@ -211,6 +221,11 @@ void lane_free(Lane &L) {
   if (L.maps_host) cudaFreeHost(L.maps_host);
   if (L.maps) cudaFree(L.maps);
   if (L.desc) cudaFree(L.desc);
+  for (int k = 0; k < 5; k++) {
+    if (L.kev[k]) cudaEventDestroy(L.kev[k]);
+    if (L.kstream[k]) cudaStreamDestroy(L.kstream[k]);
+  }
+  if (L.fork_ev) cudaEventDestroy(L.fork_ev);
   if (L.stream) cudaStreamDestroy(L.stream);
 }
 
@@ -354,15 +369,20 @@ int issue_step(ff_server *s, Lane &L, bool *issued) {
   }
   std::memset(hb + t_off, 0, 5 * sizeof(int));
   FF_CUDA(cudaMemcpyAsync(db, hb, off, cudaMemcpyHostToDevice, L.stream));
+  FF_CUDA(cudaEventRecord(L.fork_ev, L.stream));
   for (int k = 0; k < 5; k++) {
     if (!cnt[k]) continue;
     const BatchWork wl{reinterpret_cast<const int2 *>(db + e_off[k]), reinterpret_cast<const int *>(db + s_off[k]),
                        cnt[k], reinterpret_cast<int *>(db + t_off) + k};
     const int tiles = reinterpret_cast<int *>(hb + s_off[k])[cnt[k]];
     const int blocks = std::max(1, std::min(tiles, 3 * s->num_sms));
-    int rc = L.precision == FF_FP64 ? batch_pass_launch<double>(k, L.desc, L.maps, wl, blocks, kBatchSmem, L.stream)
-                                    : batch_pass_launch<float>(k, L.desc, L.maps, wl, blocks, kBatchSmem, L.stream);
+    cudaStream_t ks = L.kstream[k];
+    FF_CUDA(cudaStreamWaitEvent(ks, L.fork_ev, 0));
+    int rc = L.precision == FF_FP64 ? batch_pass_launch<double>(k, L.desc, L.maps, wl, blocks, kBatchSmem, ks)
+                                    : batch_pass_launch<float>(k, L.desc, L.maps, wl, blocks, kBatchSmem, ks);
     if (rc != FF_OK) return rc;
+    FF_CUDA(cudaEventRecord(L.kev[k], ks));
+    FF_CUDA(cudaStreamWaitEvent(L.stream, L.kev[k], 0));
     s->launches++;
   }
   FF_CUDA(cudaEventRecord(L.ring_ev[r], L.stream));

@@ -140,8 +140,9 @@ int ff_batch_tune(ff_batch *batch, void *const *density, void *const *potential,
 
 /* The tile shape pass `kind` (0..4) of grid `index` uses: W (line pairs for
  * the z passes, columns for the strided ones), ct (1: compile-time plan) and
- * tma (1: one-plane tiles loaded by TMA boxes; 0: tiles of the flattened
- * column index read straight from HBM).  Any pointer may be NULL. */
+ * tma (strided passes: 1 = one-plane tiles loaded by TMA boxes, 0 = tiles of
+ * the flattened column index read straight from HBM; z passes of runtime
+ * lengths: 1 = line blocks moved by bulk copies).  Any pointer may be NULL. */
 int ff_batch_shape(const ff_batch *batch, int index, int kind, int *W, int *ct, int *tma);
 
 /* As ff_plan_check, for the batch's device status word. */
