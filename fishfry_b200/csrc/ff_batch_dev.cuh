@@ -26,13 +26,12 @@ template <typename T> struct alignas(16) GridDesc {
 
 // ------------------------------------------------------------ column tiles
 // A strided pass over W columns of the flattened column index
-// q = plane * nh + kh, read from and written to HBM directly (no staging
-// copy): y columns are (i, kh) with rows j at stride nhp, x columns are
-// (j, kh) with rows i at stride nj*nhp.  Consecutive q of one plane are
-// contiguous, so every row access of a warp is coalesced.  Stage 0 reads
-// HBM, the middle stages run in the point-major tile, the last stage writes
-// HBM; all reads of a column precede the barrier after stage 0, so src may
-// equal dst.  The x pass runs forward DIF, the -1/k^2 filter fused with the
+// q = plane * nh + kh: y columns are (i, kh) with rows j at stride nhp, x
+// columns are (j, kh) with rows i at stride nj*nhp.  Consecutive q of one
+// plane are contiguous, so every row access of a warp is coalesced.  The tile
+// arrives by asynchronous element copies (every load of the tile in flight at
+// once), the stages run in the point-major tile, and the last stage writes
+// HBM; all reads of a column precede the first barrier, so src may equal dst.  The x pass runs forward DIF, the -1/k^2 filter fused with the
 // last DIF and first DIT stages, and the inverse DIT.  Thread t owns column
 // t % W in every stage (column-fastest item order, W divides the block).
 template <typename T, int W, bool XPASS, bool INV, int N>
@@ -50,16 +49,30 @@ __device__ __forceinline__ void cols_tile(const PassArgs<T> &a, const typename C
   const int o = valid ? (int)(q / a.nh) : 0;
   const int kh = valid ? (int)(q - (long)o * a.nh) : 0;
   const long cb = (long)o * ps + kh;
-  auto ld0 = [&](int pos, int) -> C { return valid ? src[cb + pos * rs] : mk((T)0, (T)0); };
   const auto rl = rev_last<N>(ax);
   PointTile<W, C> tl{sm};
+  {
+    // the whole tile by asynchronous element copies, all in flight at once
+    // (measured against loading stage 0 from HBM into registers: FP64 batch
+    // x pass 0.87 -> 0.68 ms, y 0.50 -> 0.44 ms)
+    const int n = N > 0 ? N : ax.n;
+    const int c = threadIdx.x % W;
+    for (int pos = threadIdx.x / W; pos < n; pos += NT / W) {
+      C *d = sm + pos * W + c;
+      if (!valid) *d = mk((T)0, (T)0);
+      else if constexpr (sizeof(C) == 16) cp_async16(d, src + cb + (long)pos * rs);
+      else cp_async8(d, src + cb + (long)pos * rs);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
   // FP64 twiddle powers by recurrence, FP32 by table loads (as the single-grid passes)
   constexpr bool TWR = sizeof(T) == 8;
   if constexpr (!XPASS) {
     auto gst = [&](int pos, int, C v) {
       if (valid) dst[cb + (long)rl(pos) * rs] = v;
     };
-    dif_all<N, INV, Map::ColFast, W, NT, false, TWR>(ax, ld0, tl, gst, W);
+    dif_all<N, INV, Map::ColFast, W, NT, false, TWR>(ax, tl, tl, gst, W);
   } else {
     auto gst = [&](int pos, int, C v) {
       if (valid) dst[cb + (long)pos * rs] = v;
@@ -84,20 +97,20 @@ __device__ __forceinline__ void cols_tile(const PassArgs<T> &a, const typename C
       constexpr int S = plan_stages(N);
       constexpr int RF = plan_radix(N, S - 1);
       if constexpr (S > 1) {
-        dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, TWR>(ax, ld0, tl, tl, W);
+        dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, TWR>(ax, tl, tl, tl, W);
         fused_filter_stage<RF, W, NT, N, C>(N, tl, tl, filt);
         __syncthreads();
         dit_ct<N, S - 2, true, Map::ColFast, W, NT, TWR>(ax, tl, gst, W);
       } else {
-        fused_filter_stage<RF, W, NT, N, C>(N, ld0, gst, filt);
+        fused_filter_stage<RF, W, NT, N, C>(N, tl, gst, filt);
       }
     } else {
       const int S = ax.nstages;
       const int n = ax.n;
-      if (S > 1) dif_rt<false, Map::ColFast, W, NT, false, TWR>(ax, S - 1, ld0, tl, tl, W);
+      if (S > 1) dif_rt<false, Map::ColFast, W, NT, false, TWR>(ax, S - 1, tl, tl, tl, W);
       with_radix(ax.radix[S - 1], [&](auto tag) {
         constexpr int R = decltype(tag)::value;
-        if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, ld0, gst, filt);
+        if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, tl, gst, filt);
         else fused_filter_stage<R, W, NT, 0, C>(n, tl, tl, filt);
       });
       __syncthreads();

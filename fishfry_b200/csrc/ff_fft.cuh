@@ -607,6 +607,20 @@ __device__ __forceinline__ void l2_prefetch(const void *src, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 
+// Element copies from global to shared memory that complete asynchronously
+// (all of a thread's copies are in flight together); 16 bytes (.cg, L2 only)
+// or 8 bytes (.ca); addresses aligned to the size.  cp_async_wait_all waits
+// for this thread's copies; a barrier then publishes them to the block.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Device-side status word values (plan status buffer).
 enum : int { kDevOk = 0, kDevTmaTimeout = 1, kDevDepTimeout = 2 };
 
