@@ -30,7 +30,7 @@ EXPORTS = [
     "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_status_string",
     "ff_last_error", "ff_version",
     "ff_batch_create", "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
-    "ff_batch_destroy",
+    "ff_batch_destroy", "ff_batch_radices",
     "ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_next", "ff_server_fetch",
     "ff_server_release",
     "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy",
@@ -103,6 +103,7 @@ def _declare(L):
     L.ff_batch_tune.argtypes = [vp, pp, pp, vp, ctypes.c_int]
     L.ff_batch_shape.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip, ip]
     L.ff_batch_check.argtypes = [vp, vp]
+    L.ff_batch_radices.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
     L.ff_batch_destroy.argtypes = [vp]
     L.ff_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.ff_server_submit.argtypes = [vp, i3, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]
@@ -121,7 +122,7 @@ def _declare(L):
     for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
                  "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_batch_create",
                  "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
-                 "ff_batch_destroy"):
+                 "ff_batch_destroy", "ff_batch_radices"):
         getattr(L, name).restype = ctypes.c_int
 
 

@@ -152,6 +152,13 @@ class Batch:
                                    ctypes.byref(tma)), "ff_batch_shape")
         return W.value, ct.value, tma.value
 
+    def radices(self, index, axis):
+        """Radix split (DIF stage order) of grid `index` on axis 0=x, 1=y, 2=z."""
+        r = (ctypes.c_int * 16)()
+        cnt = ctypes.c_int()
+        check(lib().ff_batch_radices(self._h, int(index), int(axis), r, ctypes.byref(cnt)), "ff_batch_radices")
+        return list(r)[:cnt.value]
+
     def check(self, stream=None):
         check(lib().ff_batch_check(self._h, _stream(stream)), "ff_batch_check")
 

@@ -63,6 +63,10 @@ struct ff_batch {
   int blocks[5] = {};
   size_t smem[5] = {};
   bool desc_dirty = true;
+  // axis tables by (length, radix order); default orders live in dmem, other
+  // orders (from the tuner) in their own allocations
+  std::map<std::pair<int, int>, std::pair<AxisDev<double2>, AxisDev<float2>>> tables;
+  std::vector<void *> extra;
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -122,6 +126,7 @@ bool batch_z_bulk_ok(int precision, int nk) {
 
 bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const TileShape &s) {
   if (s.W < 1) return false;
+  if (s.order != 0 && (s.ct || kind > 2 || batch_radix_order(batch_axis_len(g, kind), s.order).empty())) return false;
   if (s.ct && !batch_special_n(batch_axis_len(g, kind))) return false;
   if (kind != 0 && kind != 4) {
     const int w1 = 128 / (precision == FF_FP64 ? 16 : 8);
@@ -185,7 +190,23 @@ size_t batch_axis_bytes(int n, int precision) {
   return r(n * csz) + (precision == FF_FP64 ? 0 : r(n * sizeof(double2))) + 2 * r(n * sizeof(int));
 }
 
-int batch_axis_build(int n, int precision, void *mem, AxisDev<double2> *ad, AxisDev<float2> *af, cudaStream_t st) {
+std::vector<int> batch_radix_order(int n, int order) {
+  const std::vector<int> def = plan_factor_radices(n);
+  std::vector<int> r = def;
+  if (order == 1) {
+    std::reverse(r.begin(), r.end());
+  } else if (order == 2) {
+    std::stable_partition(r.begin(), r.end(), [](int x) { return x == 5 || x == 3; });
+  } else if (order != 0) {
+    return {};
+  }
+  for (int q = 0; q < order; q++)
+    if (batch_radix_order(n, q) == r) return {};
+  return r;
+}
+
+int batch_axis_build(int n, int precision, int order, void *mem, AxisDev<double2> *ad, AxisDev<float2> *af,
+                     cudaStream_t st) {
   const size_t csz = precision == FF_FP64 ? 16 : 8;
   auto r = [](size_t b) { return (b + 255) & ~size_t(255); };
   char *base = static_cast<char *>(mem);
@@ -193,7 +214,8 @@ int batch_axis_build(int n, int precision, void *mem, AxisDev<double2> *ad, Axis
   const size_t o_tw64 = precision == FF_FP64 ? o_tw : r(n * csz);
   const size_t o_rev = precision == FF_FP64 ? r(n * csz) : o_tw64 + r(n * sizeof(double2));
   const size_t o_ipos = o_rev + r(n * sizeof(int));
-  const std::vector<int> radix = plan_factor_radices(n);
+  const std::vector<int> radix = batch_radix_order(n, order);
+  if (radix.empty()) return set_error(FF_ERR_INVALID, "radix order %d of length %d", order, n);
   const std::vector<int> rev = plan_digit_reversal(n, radix);
   std::vector<int> ipos(n);
   for (int q = 0; q < n; q++) ipos[rev[q]] = q;
@@ -276,7 +298,37 @@ namespace {
 
 // Work lists, block counts and shared memory of every pass from the grids'
 // current shapes; uploads lists and descriptors (synchronously).
+// Points every grid's axes at the tables of the radix order its owning pass
+// uses (z: pass 0, y: pass 1, x: pass 2), building missing ones.
+int apply_orders(ff_batch *b) {
+  static const int owner[3] = {2, 1, 0};   // axis d is owned by pass owner[d]
+  for (auto &g : b->grids) {
+    for (int d = 0; d < 3; d++) {
+      const int order = g.shape[owner[d]].order;
+      auto key = std::make_pair(g.n[d], order);
+      auto it = b->tables.find(key);
+      if (it == b->tables.end()) {
+        void *mem = nullptr;
+        FF_CUDA(cudaMalloc(&mem, batch_axis_bytes(g.n[d], b->precision)));
+        b->extra.push_back(mem);
+        AxisDev<double2> ad;
+        AxisDev<float2> af;
+        const int rc = batch_axis_build(g.n[d], b->precision, order, mem, &ad, &af, b->cap);
+        if (rc != FF_OK) return rc;
+        it = b->tables.emplace(key, std::make_pair(ad, af)).first;
+      }
+      g.axd[d] = it->second.first;
+      g.axf[d] = it->second.second;
+    }
+  }
+  return FF_OK;
+}
+
 int build_work(ff_batch *b) {
+  {
+    const int rc = apply_orders(b);
+    if (rc != FF_OK) return rc;
+  }
   for (int k = 0; k < 5; k++) {
     std::vector<int2> ent(b->count);
     std::vector<int> start(b->count + 1, 0);
@@ -477,8 +529,9 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
     if (rc != FF_OK) break;
     AxisDev<double2> ad;
     AxisDev<float2> af;
-    rc = batch_axis_build(t.first, precision, base + t.second, &ad, &af, b->cap);
+    rc = batch_axis_build(t.first, precision, 0, base + t.second, &ad, &af, b->cap);
     axes[t.first] = std::make_pair(ad, af);
+    b->tables[std::make_pair(t.first, 0)] = std::make_pair(ad, af);
   }
   b->grids.resize(count);
   b->bytes.resize(count);
@@ -517,6 +570,15 @@ int ff_batch_shape(const ff_batch *b, int index, int kind, int *W, int *ct, int 
   if (W) *W = b->grids[index].shape[kind].W;
   if (ct) *ct = b->grids[index].shape[kind].ct;
   if (tma) *tma = b->grids[index].shape[kind].tma;
+  return FF_OK;
+}
+
+int ff_batch_radices(const ff_batch *b, int index, int axis, int radix[16], int *count) {
+  if (!b || index < 0 || index >= b->count || axis < 0 || axis > 2 || !radix || !count)
+    return set_error(FF_ERR_INVALID, "ff_batch_radices: bad argument");
+  const AxisDev<double2> &ax = b->grids[index].axd[axis];
+  *count = ax.nstages;
+  for (int q = 0; q < ax.nstages; q++) radix[q] = ax.radix[q];
   return FF_OK;
 }
 
@@ -582,18 +644,35 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
       for (int ct = batch_special_n(n) ? 1 : 0; ct >= 0; ct--) {
         if (k == 0 || k == 4) {
           for (int W : {std::max(1, d.W / 2), d.W, d.W * 2}) {
-            cand.push_back(TileShape{W, ct, 0});
-            if (!ct) cand.push_back(TileShape{W, 0, 1});
+            cand.push_back(TileShape{W, ct, 0, 0});
+            if (!ct) cand.push_back(TileShape{W, 0, 1, 0});
           }
         } else {
           const int w1 = 128 / (int)b->csz;
-          for (int m : {1, 2, 4}) cand.push_back(TileShape{m * w1, ct, 0});
-          cand.push_back(TileShape{w1, ct, 1});
+          for (int m : {1, 2, 4}) cand.push_back(TileShape{m * w1, ct, 0, 0});
+          cand.push_back(TileShape{w1, ct, 1, 0});
         }
       }
+      // runtime plans of the pass that owns the axis: every radix order too
+      if (k <= 2) {
+        const size_t base_count = cand.size();
+        for (int order = 1; order < kBatchOrders; order++) {
+          if (batch_radix_order(n, order).empty()) continue;
+          for (size_t q = 0; q < base_count; q++)
+            if (!cand[q].ct) {
+              TileShape c = cand[q];
+              c.order = order;
+              cand.push_back(c);
+            }
+        }
+      }
+      // the shape in use is timed first and kept unless a candidate beats it
+      // by more than 3 % (passes of near-equal candidates differ by noise)
       TileShape best = ref.shape[k];
       float best_ms = 1e30f;
-      for (const TileShape &c : cand) {
+      cand.insert(cand.begin(), best);
+      for (size_t ci = 0; ci < cand.size(); ci++) {
+        const TileShape &c = cand[ci];
         bool ok = true;
         for (const auto &g : b->grids)
           if (batch_axis_len(g, k) == n && !batch_shape_valid(b->precision, g, k, c)) ok = false;
@@ -605,7 +684,7 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
         float ms = 0;
         if (rc == FF_OK) rc = time_pass(b, k, st, reps, &ms);
         if (rc != FF_OK) return rc;
-        if (ms < best_ms) {
+        if (ci == 0 || ms < 0.97f * best_ms) {
           best_ms = ms;
           best = c;
         }
@@ -631,6 +710,7 @@ int ff_batch_destroy(ff_batch *b) {
   if (b->desc_host) cudaFreeHost(b->desc_host);
   if (b->maps_host) cudaFreeHost(b->maps_host);
   int rc = FF_OK;
+  for (void *m : b->extra) cudaFree(m);
   if (b->dmem && cudaFree(b->dmem) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_destroy: cudaFree failed");
   delete b;
   return rc;

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <vector>
 
 #include "ff_fft.cuh"
 
@@ -55,11 +56,21 @@ struct BatchWork {
 // tma = 0 is W columns of the flattened (plane, kh) index, read straight from
 // HBM.  z passes of runtime lengths: tma = 1 moves the line blocks by bulk
 // copies (compile-time lengths always do).
+// order (runtime plans of the owning pass only: z fwd for the z axis, y fwd
+// for y, x for x): the radix split of the axis, as batch_radix_order numbers
+// it; 0 is the default plan order.
 struct TileShape {
   int W;
   int ct;
   int tma;
+  int order;
 };
+
+// Radix orders the tuner tries for a runtime length: 0 the default plan
+// (8s, one 4 or 2, 5s, 3s), 1 the same radices reversed, 2 the odd radices
+// first.  Empty if the order repeats a lower-numbered one.
+constexpr int kBatchOrders = 3;
+std::vector<int> batch_radix_order(int n, int order);
 
 // Shared memory of one tile (bytes, with alignment slack).
 inline size_t batch_tile_smem(int kind, int n_axis, int nk, int nhp, int W, size_t csz) {
@@ -118,7 +129,8 @@ TileShape batch_default_shape(int precision, const BatchGridHost &g, int kind);
 TileShape batch_shape_for(int precision, const BatchGridHost &g, int kind);
 // Device bytes of one axis's tables, and their construction at mem (waits for st).
 size_t batch_axis_bytes(int n, int precision);
-int batch_axis_build(int n, int precision, void *mem, AxisDev<double2> *ad, AxisDev<float2> *af, cudaStream_t st);
+int batch_axis_build(int n, int precision, int order, void *mem, AxisDev<double2> *ad, AxisDev<float2> *af,
+                     cudaStream_t st);
 // Dimensions, wavenumber scales (lo/hi: 3 values or NULL), nh/nhp, 1/N.
 void batch_grid_init(BatchGridHost &h, const int n[3], const double *lo, const double *hi, int precision);
 size_t batch_grid_bytes(const BatchGridHost &h, int precision);

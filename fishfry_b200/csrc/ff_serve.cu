@@ -24,6 +24,7 @@
 #include <map>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "ff_batch.hpp"
@@ -153,7 +154,7 @@ struct ff_server {
   int *status = nullptr;
   cudaStream_t copy = nullptr, fetch = nullptr, setup = nullptr;
   Lane lane[2];
-  std::map<std::pair<int, int>, AxisEntry> axes;   // (n, precision)
+  std::map<std::tuple<int, int, int>, AxisEntry> axes;   // (n, precision, radix order)
   std::map<uint64_t, Request> reqs;
   std::deque<uint64_t> pending;
   std::vector<uint64_t> active;   // admitted, not yet done (loading or running)
@@ -229,13 +230,13 @@ void lane_free(Lane &L) {
   if (L.stream) cudaStreamDestroy(L.stream);
 }
 
-int axis_for(ff_server *s, int n, int precision, AxisEntry **out) {
-  auto key = std::make_pair(n, precision);
+int axis_for(ff_server *s, int n, int precision, int order, AxisEntry **out) {
+  auto key = std::make_tuple(n, precision, order);
   auto it = s->axes.find(key);
   if (it == s->axes.end()) {
     AxisEntry e;
     FF_CUDA(cudaMalloc(&e.mem, batch_axis_bytes(n, precision)));
-    int rc = batch_axis_build(n, precision, e.mem, &e.ad, &e.af, s->setup);
+    int rc = batch_axis_build(n, precision, order, e.mem, &e.ad, &e.af, s->setup);
     if (rc != FF_OK) {
       cudaFree(e.mem);
       return rc;
@@ -282,20 +283,20 @@ int admit(ff_server *s) {
     q.off_p = op;
     q.slot = L.free_slots.back();
     L.free_slots.pop_back();
-    AxisEntry *ax[3];
-    for (int d = 0; d < 3; d++) {
-      int rc = axis_for(s, q.n[d], q.precision, &ax[d]);
-      if (rc != FF_OK) return rc;
-    }
     batch_grid_init(q.g, q.n, nullptr, nullptr, q.precision);
+    for (int k = 0; k < 5; k++) q.g.shape[k] = batch_shape_for(q.precision, q.g, k);
+    // axis d's tables in the radix order of the pass that owns it (z: 0, y: 1, x: 2)
+    static const int owner[3] = {2, 1, 0};
     for (int d = 0; d < 3; d++) {
-      q.g.axd[d] = ax[d]->ad;
-      q.g.axf[d] = ax[d]->af;
+      AxisEntry *ax = nullptr;
+      int rc = axis_for(s, q.n[d], q.precision, q.g.shape[owner[d]].order, &ax);
+      if (rc != FF_OK) return rc;
+      q.g.axd[d] = ax->ad;
+      q.g.axf[d] = ax->af;
     }
     q.g.status = s->status;
     q.g.density = s->arena_base + q.off_d;
     q.g.potential = s->arena_base + q.off_p;
-    for (int k = 0; k < 5; k++) q.g.shape[k] = batch_shape_for(q.precision, q.g, k);
     const size_t esz = q.precision == FF_FP64 ? 8 : 4;
     const size_t fbytes = (size_t)q.n[0] * q.n[1] * q.n[2] * esz;
     FF_CUDA(cudaMemcpyAsync(q.g.density, q.f, fbytes, q.f_on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,

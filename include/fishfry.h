@@ -132,7 +132,8 @@ int ff_batch_solve(ff_batch *batch, void *const *density, void *const *potential
 
 /* Autotuner: times each pass with every candidate tile shape for each axis
  * length of the batch (z passes: line pairs per tile; strided passes:
- * columns per tile; compile-time or runtime radix plan) and keeps the fastest.
+ * columns per tile; compile-time or runtime radix plan; for runtime plans, the
+ * order of the radices) and keeps the fastest.
  * Results are also remembered for batches created later in this process.
  * The buffers are overwritten (zeroed, then used as scratch); initialise the
  * densities after tuning.  reps: timed launches per candidate (median). */
@@ -144,6 +145,11 @@ int ff_batch_tune(ff_batch *batch, void *const *density, void *const *potential,
  * the flattened column index read straight from HBM; z passes of runtime
  * lengths: 1 = line blocks moved by bulk copies).  Any pointer may be NULL. */
 int ff_batch_shape(const ff_batch *batch, int index, int kind, int *W, int *ct, int *tma);
+
+/* The radix split (DIF stage radices, first stage first) grid `index` uses
+ * on axis `axis` (0 = x, 1 = y, 2 = z): the tuner may reorder the radices of a
+ * runtime-plan length.  radix has room for 16 entries. */
+int ff_batch_radices(const ff_batch *batch, int index, int axis, int radix[16], int *count);
 
 /* As ff_plan_check, for the batch's device status word. */
 int ff_batch_check(ff_batch *batch, void *stream);

@@ -117,10 +117,50 @@ def test_batch_tuned_shapes_keep_parity(torch_cuda, ff, oracle, precision, tol):
             assert W >= 1 and ct in (0, 1) and tma in (0, 1)
             if kind in (1, 2, 3):
                 assert (W * csz) % 128 == 0
+    # the radix split of every axis is a reordering of the default one
+    for g, n in enumerate(batch.dims):
+        for axis in range(3):
+            r = batch.radices(g, axis)
+            assert sorted(r) == sorted(default_radices(n[axis])) and int(np.prod(r)) == n[axis], (g, axis, r)
     fs = init_all(ff, batch, d, modes_for(ff), precision)
     batch.solve(d, p)
     for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
         assert rel_l2(phi, oracle.solve(f)) <= tol, (g, batch.dims[g])
+
+
+def default_radices(n):
+    """The default plan's radices: 8s while three factors of 2 remain, one 4 or
+    2, then 5s, then 3s; a length of 1 is one stage of radix 1."""
+    twos = fives = threes = 0
+    m = n
+    while m > 1 and m % 2 == 0:
+        m //= 2
+        twos += 1
+    while m > 1 and m % 5 == 0:
+        m //= 5
+        fives += 1
+    while m > 1 and m % 3 == 0:
+        m //= 3
+        threes += 1
+    r = [8] * (twos // 3) + ([4] if twos % 3 == 2 else [2] if twos % 3 == 1 else []) + [5] * fives + [3] * threes
+    return r or [1]
+
+
+def test_batch_tuner_reorders_radices_of_runtime_lengths(torch_cuda, ff, oracle):
+    """Lengths with mixed radices (runtime plans) get their radix order tuned;
+    whatever order wins, results match the oracle."""
+    dims = [(60, 90, 150), (150, 60, 90), (90, 150, 60), (45, 120, 100)]
+    batch = ff.Batch(dims)
+    d, p = make_buffers(torch_cuda, batch, 0)
+    batch.tune(d, p, reps=1)
+    for g, n in enumerate(dims):
+        for axis in range(3):
+            r = batch.radices(g, axis)
+            assert sorted(r) == sorted(default_radices(n[axis])), (g, axis, r)
+    fs = init_all(ff, batch, d, modes_for(ff, 31), 0)
+    batch.solve(d, p)
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL, (g, dims[g])
 
 
 def test_batch_of_256_seeded_grids(torch_cuda, ff, oracle):
