@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kZThreads, (KIND == 0 || KIND == 4) ? FF_BATCH
       // later (ticket t + gridDim.x) into L2, where its inbound copy (bulk
       // copy or thread loads) will find them
       const int t2 = t + (int)gridDim.x;
-      if (threadIdx.x == 0 && t2 < total) {
+      if (threadIdx.x == 32 && t2 < total) {   // not thread 0, which issues the tile's own copy
         int a2 = lo, b2 = wl.nentry - 1;
         while (a2 < b2) {
           const int mid = (a2 + b2 + 1) >> 1;
