@@ -161,3 +161,20 @@ def test_reference_printout_golden():
                     assert abs(g - want) <= 1e-4 * want
             seen += 1
     assert seen >= 1
+
+
+def test_oracle_general_box_single_mode(oracle):
+    """The oracle's wavenumber scale for a box of side L (hi one cell short):
+    a single mode cos(2*pi*k*x/L) solves to -cos(...)/(2*pi*k/L)^2."""
+    import numpy as np
+    n = (24, 20, 16)
+    L = (3.0, 10.0, 1.5)
+    lo = [0.0, -1.0, 2.5]
+    hi = [lo[a] + L[a] * (n[a] - 1) / n[a] for a in range(3)]
+    k = (2, 1, 3)
+    x = [lo[a] + np.arange(n[a]) * L[a] / n[a] for a in range(3)]
+    X, Y, Z = np.meshgrid(x[0], x[1], x[2], indexing="ij")
+    arg = 2 * np.pi * (k[0] * X / L[0] + k[1] * Y / L[1] + k[2] * Z / L[2])
+    k2 = sum((2 * np.pi * k[a] / L[a]) ** 2 for a in range(3))
+    phi = oracle.solve(np.cos(arg), lo, hi)
+    assert np.abs(phi + np.cos(arg) / k2).max() <= 1e-13 * np.abs(np.cos(arg) / k2).max()

@@ -270,3 +270,60 @@ def test_fused_passes_parity(torch_cuda, ff, oracle, n, monkeypatch):
     f = d[:N].cpu().numpy().reshape(n)
     plan.solve(d, p, timed=True)
     assert rel_l2(p[:N].cpu().numpy().reshape(n), oracle.solve(f)) <= FP64_TOL
+
+
+def box_bounds(n, L, lo0=(0.0, -1.0, 2.5)):
+    """Bounds of a periodic box of side L[a] sampled at n[a] points, with hi one
+    cell short of the period as the reference's harness passes them
+    (FishFry.hpp:133-134); the wavenumber scale is then 2*pi/L."""
+    lo = [lo0[a] for a in range(3)]
+    hi = [lo0[a] + L[a] * (n[a] - 1) / n[a] for a in range(3)]
+    return lo, hi
+
+
+@pytest.mark.parametrize("n,L", [((48, 40, 64), (3.0, 10.0, 1.5)), ((30, 45, 50), (1.0, 2.0, 7.0)),
+                                 ((256, 8, 12), (0.5, 0.5, 0.5))])
+def test_general_box_matches_oracle_and_mode_solution(torch_cuda, ff, oracle, n, L):
+    """Boxes other than the reference's 2*pi cube (ParisPencil.cpp:9-11 derives
+    the wavenumber scale from lo/hi): against the oracle on the same bounds,
+    and against the exact solution of one Fourier mode,
+    f = cos(2*pi*(kx*x/Lx + ky*y/Ly + kz*z/Lz)) -> phi = -f / |2*pi*k/L|^2."""
+    lo, hi = box_bounds(n, L)
+    k = (2, 1, 3)
+    x = [lo[a] + np.arange(n[a]) * L[a] / n[a] for a in range(3)]
+    X, Y, Z = np.meshgrid(x[0], x[1], x[2], indexing="ij")
+    arg = 2 * np.pi * (k[0] * X / L[0] + k[1] * Y / L[1] + k[2] * Z / L[2])
+    rng = np.random.default_rng(5)
+    f = np.cos(arg) + 0.1 * rng.standard_normal(n)
+    f -= f.mean()
+    plan = ff.Plan(n, lo, hi)
+    d = torch_cuda.zeros(plan.nbytes // 8, dtype=torch_cuda.float64, device="cuda")
+    p = torch_cuda.empty_like(d)
+    N = f.size
+    d[:N] = torch_cuda.from_numpy(f.ravel()).cuda()
+    plan.solve(d, p)
+    phi = p[:N].cpu().numpy().reshape(n)
+    assert rel_l2(phi, oracle.solve(f, lo, hi)) <= FP64_TOL
+    # the single mode alone
+    k2 = sum((2 * np.pi * k[a] / L[a]) ** 2 for a in range(3))
+    d[:N] = torch_cuda.from_numpy(np.cos(arg).ravel()).cuda()
+    plan.solve(d, p)
+    phi1 = p[:N].cpu().numpy().reshape(n)
+    assert rel_l2(phi1, -np.cos(arg) / k2) <= 1e-12
+
+
+def test_general_box_in_a_batch(torch_cuda, ff, oracle):
+    dims = [(48, 40, 64), (30, 45, 50)]
+    Ls = [(3.0, 10.0, 1.5), (1.0, 2.0, 7.0)]
+    bounds = [box_bounds(n, L) for n, L in zip(dims, Ls)]
+    batch = ff.Batch(dims, lo=[b[0] for b in bounds], hi=[b[1] for b in bounds])
+    rng = np.random.default_rng(8)
+    fs = [rng.standard_normal(n) for n in dims]
+    d = [torch_cuda.zeros(nb // 8, dtype=torch_cuda.float64, device="cuda") for nb in batch.nbytes]
+    p = [torch_cuda.empty_like(x) for x in d]
+    for g, f in enumerate(fs):
+        d[g][:f.size] = torch_cuda.from_numpy(f.ravel()).cuda()
+    batch.solve(d, p)
+    for g, (f, (lo, hi)) in enumerate(zip(fs, bounds)):
+        phi = p[g][:f.size].cpu().numpy().reshape(dims[g])
+        assert rel_l2(phi, oracle.solve(f, lo, hi)) <= FP64_TOL, g
