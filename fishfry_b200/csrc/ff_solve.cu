@@ -35,7 +35,7 @@ namespace ff {
 
 // Lengths with compile-time specialised kernels (fully unrolled stages);
 // every other length runs the same kernels with the plan read at run time.
-#define FF_FOR_EACH_SPECIAL_N(X) X(256) X(512) X(1024)
+#define FF_FOR_EACH_SPECIAL_N(X) X(64) X(128) X(256) X(512) X(1024)
 
 // ------------------------------------------------- unfused pass kernels
 // (one launch per pass; used when the fused passes are switched off)
