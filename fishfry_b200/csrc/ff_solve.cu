@@ -27,6 +27,7 @@
 #include <cstring>
 #include <vector>
 
+#include "ff_bluestein.hpp"
 #include "ff_fft.cuh"
 #include "ff_tiles.cuh"
 #include "ff_status.hpp"
@@ -480,6 +481,13 @@ struct ff_plan {
   int l2_ahead;        // forward z pass: L2 prefetch distance in blocks (0: off)
   StridedCfg ycfg, xcfg;
   FusedCfg fwd, inv;
+  // axes with a prime factor above 5: padded convolution length M (0 for a
+  // 2^a 3^b 5^c axis), their tables, and the launch shape of each pass kind
+  // (0 z fwd, 1 y fwd, 2 x, 3 y inv, 4 z inv) that transforms such an axis
+  int bsM[3];
+  BsAxis<double2> bsd[3];
+  BsAxis<float2> bsf[3];
+  BsCfg bscfg[5];
   cudaEvent_t ev[FF_MAX_PHASES + 1];
 };
 
@@ -621,6 +629,14 @@ template <typename T> static int configure(ff_plan *p) {
   using C = typename Cplx<T>::type;
   const size_t csz = sizeof(C);
   const int ni = p->n[0], nj = p->n[1], nk = p->n[2];
+  int rc = FF_OK;
+  // passes along an axis with a prime factor above 5 (pass kind -> axis)
+  const int axis_of_kind[5] = {2, 1, 0, 1, 2};
+  for (int kind = 0; kind < 5 && rc == FF_OK; kind++)
+    if (p->bsM[axis_of_kind[kind]])
+      rc = bs_configure<T>(kind, ni, nj, p->nh, p->bsM[axis_of_kind[kind]], &p->bscfg[kind]);
+  if (rc != FF_OK) return rc;
+  const bool any_bs = p->bsM[0] || p->bsM[1] || p->bsM[2];
   // z tiles: W line pairs, two line-major buffers of pitch P, ~64 KB per block
   const int align = csz == 16 ? 8 : 16;
   p->zN = special_n(nk);
@@ -637,15 +653,18 @@ template <typename T> static int configure(ff_plan *p) {
   // that is not the last (the bulk-fed tiles stage their input in the buffer
   // the last stage writes)
   p->zbulk = p->zN > 0 || ((nk * sizeof(T)) % 16 == 0 && plan_stages(nk) >= 2);
-  int rc = allow_dyn_smem(zfwd_kernel<T>(p->zN, p->zbulk), nullptr);
-  if (rc == FF_OK) rc = allow_dyn_smem(zinv_kernel<T>(p->zN, p->zbulk), nullptr);
-  if (rc != FF_OK) return rc;
+  if (!p->bsM[2]) {
+    rc = allow_dyn_smem(zfwd_kernel<T>(p->zN, p->zbulk), nullptr);
+    if (rc == FF_OK) rc = allow_dyn_smem(zinv_kernel<T>(p->zN, p->zbulk), nullptr);
+    if (rc != FF_OK) return rc;
+  }
   // strided tiles: W 128-byte columns x n rows, one per block
   const int W = 128 / (int)csz;
   const int ktiles = (p->nh + W - 1) / W;
   for (int kind = 0; kind < 3; kind++) {
     StridedCfg &cfg = kind == 2 ? p->xcfg : p->ycfg;
     const int n = kind == 2 ? ni : nj;
+    if (p->bsM[kind == 2 ? 0 : 1]) continue;
     cfg.N = special_n(n);
     cfg.W = W;
     cfg.box_rows = largest_divisor_at_most(n, 256, 1);
@@ -657,9 +676,10 @@ template <typename T> static int configure(ff_plan *p) {
     if (cfg.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "no tile shape for an axis of %d points", n);
     cfg.grid = (kind == 2 ? nj : ni) * ktiles * pair;
   }
-  // fused passes: persistent blocks over the in-order tile queue
+  // fused passes: persistent blocks over the in-order tile queue (not with
+  // Bluestein axes)
   const int zpp = (nj + 2 * p->zW - 1) / (2 * p->zW);   // z tiles per plane (pairs never cross planes)
-  for (int dir = 0; dir < 2; dir++) {
+  for (int dir = 0; dir < 2 && !any_bs; dir++) {
     FusedCfg &fc = dir == 0 ? p->fwd : p->inv;
     fused_pair(nk, nj, &fc.NZ, &fc.NY);
     fc.smem = std::max(p->zsmem, p->ycfg.smem);
@@ -697,7 +717,7 @@ template <typename T> static int configure(ff_plan *p) {
   p->l2_ahead = ahead ? std::max(0, atoi(ahead)) : 3 * p->num_sms;
   const char *mode = getenv("FF_PASSES");
   // the fused passes hold a whole y tile per block: not for 1024-point y lines
-  p->fused = mode && strcmp(mode, "3") == 0 && p->ycfg.N != 1024;
+  p->fused = mode && strcmp(mode, "3") == 0 && p->ycfg.N != 1024 && !any_bs;
   return FF_OK;
 }
 
@@ -772,9 +792,14 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
   C *Ds = reinterpret_cast<C *>(density);
   C *Ps = reinterpret_cast<C *>(potential);
   CUtensorMap ymapP, xmapP;
-  int rc = spectrum_map<T>(p, potential, p->ycfg, false, &ymapP);
-  if (rc == FF_OK) rc = spectrum_map<T>(p, potential, p->xcfg, true, &xmapP);
+  int rc = FF_OK;
+  if (!p->bsM[1]) rc = spectrum_map<T>(p, potential, p->ycfg, false, &ymapP);
+  if (rc == FF_OK && !p->bsM[0]) rc = spectrum_map<T>(p, potential, p->xcfg, true, &xmapP);
   if (rc != FF_OK) return rc;
+  auto bsax = [&](int d) -> const BsAxis<C> & {
+    if constexpr (sizeof(T) == 8) return p->bsd[d];
+    else return p->bsf[d];
+  };
   int ev = 0;
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
   if (p->fused) {
@@ -795,20 +820,46 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
     return FF_OK;
   }
-  zfwd_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(D, Ps, a, p->zW, p->zP);
-  FF_CUDA(cudaGetLastError());
+  // each pass through the Bluestein kernels where its axis needs them
+  if (p->bsM[2]) {
+    rc = bs_launch<T>(0, D, Ps, a, bsax(2), p->bscfg[0], st);
+    if (rc != FF_OK) return rc;
+  } else {
+    zfwd_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(D, Ps, a, p->zW, p->zP);
+    FF_CUDA(cudaGetLastError());
+  }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
-  strided_kernel<T>(0, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ps, a, p->ycfg.box_rows);
-  FF_CUDA(cudaGetLastError());
+  if (p->bsM[1]) {
+    rc = bs_launch<T>(1, Ps, Ps, a, bsax(1), p->bscfg[1], st);
+    if (rc != FF_OK) return rc;
+  } else {
+    strided_kernel<T>(0, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ps, a, p->ycfg.box_rows);
+    FF_CUDA(cudaGetLastError());
+  }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
-  strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
-  FF_CUDA(cudaGetLastError());
+  if (p->bsM[0]) {
+    rc = bs_launch<T>(2, Ps, Ps, a, bsax(0), p->bscfg[2], st);
+    if (rc != FF_OK) return rc;
+  } else {
+    strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
+    FF_CUDA(cudaGetLastError());
+  }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
-  strided_kernel<T>(1, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ds, a, p->ycfg.box_rows);
-  FF_CUDA(cudaGetLastError());
+  if (p->bsM[1]) {
+    rc = bs_launch<T>(3, Ps, Ds, a, bsax(1), p->bscfg[3], st);
+    if (rc != FF_OK) return rc;
+  } else {
+    strided_kernel<T>(1, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ds, a, p->ycfg.box_rows);
+    FF_CUDA(cudaGetLastError());
+  }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
-  zinv_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(Ds, P, a, p->zW, p->zP);
-  FF_CUDA(cudaGetLastError());
+  if (p->bsM[2]) {
+    rc = bs_launch<T>(4, Ds, P, a, bsax(2), p->bscfg[4], st);
+    if (rc != FF_OK) return rc;
+  } else {
+    zinv_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(Ds, P, a, p->zW, p->zP);
+    FF_CUDA(cudaGetLastError());
+  }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
   return FF_OK;
 }
@@ -874,9 +925,8 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
     return set_error(FF_ERR_INVALID, "ff_plan_create: precision %d is neither FF_FP64 nor FF_FP32", precision);
   for (int d = 0; d < 3; d++) {
     if (n[d] < 1) return set_error(FF_ERR_INVALID, "ff_plan_create: n[%d] = %d < 1", d, n[d]);
-    if (n[d] > FF_MAX_AXIS || !smooth235(n[d]))
-      return set_error(FF_ERR_UNSUPPORTED, "ff_plan_create: n[%d] = %d is not 2^a 3^b 5^c <= %d", d, n[d],
-                       FF_MAX_AXIS);
+    if (n[d] > FF_MAX_AXIS)
+      return set_error(FF_ERR_UNSUPPORTED, "ff_plan_create: n[%d] = %d is above %d", d, n[d], FF_MAX_AXIS);
     if (!(hi[d] > lo[d]) && n[d] > 1)
       return set_error(FF_ERR_INVALID, "ff_plan_create: hi[%d] <= lo[%d]", d, d);
   }
@@ -902,24 +952,33 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
     return set_error(FF_ERR_CUDA, "ff_plan_create: no current CUDA device");
   }
 
-  // device tables: per axis tw (n complex), rev and ipos (n ints); kk per
-  // axis; one status word
+  // device tables: per axis tw (L complex), rev and ipos (L ints) of the
+  // axis's transform length L (n, or the padded M of a Bluestein axis), the
+  // chirp (n) and kernel transform (M) of a Bluestein axis; kk per axis; one
+  // status word
   std::vector<int> radix[3], rev[3];
+  int len[3];
   size_t off = 0;
-  size_t o_tw[3], o_tw64[3], o_rev[3], o_ipos[3], o_kk[3];
+  size_t o_tw[3], o_tw64[3], o_rev[3], o_ipos[3], o_kk[3], o_chirp[3] = {0, 0, 0}, o_ghat[3] = {0, 0, 0};
   auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~size_t(255); return o; };
   for (int d = 0; d < 3; d++) {
-    radix[d] = plan_factor_radices(n[d]);
+    p->bsM[d] = smooth235(n[d]) ? 0 : bs_padded_length(n[d]);
+    const int L = len[d] = p->bsM[d] ? p->bsM[d] : n[d];
+    radix[d] = plan_factor_radices(L);
     if ((int)radix[d].size() > kMaxStages) {
       delete p;
       return set_error(FF_ERR_UNSUPPORTED, "ff_plan_create: too many stages");
     }
-    rev[d] = plan_digit_reversal(n[d], radix[d]);
-    o_tw[d] = take(n[d] * csz);
-    o_tw64[d] = precision == FF_FP64 ? o_tw[d] : take(n[d] * sizeof(double2));
-    o_rev[d] = take(n[d] * sizeof(int));
-    o_ipos[d] = take(n[d] * sizeof(int));
+    rev[d] = plan_digit_reversal(L, radix[d]);
+    o_tw[d] = take(L * csz);
+    o_tw64[d] = precision == FF_FP64 ? o_tw[d] : take(L * sizeof(double2));
+    o_rev[d] = take(L * sizeof(int));
+    o_ipos[d] = take(L * sizeof(int));
     o_kk[d] = take((d == 2 ? p->nh : n[d]) * sizeof(double));
+    if (p->bsM[d]) {
+      o_chirp[d] = take(n[d] * csz);
+      o_ghat[d] = take(L * csz);
+    }
   }
   const size_t o_status = take(sizeof(int));
   const size_t o_counters = take((2 + 2 * (size_t)n[0]) * sizeof(int));
@@ -942,21 +1001,22 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
   int rc = FF_OK;
   if (cudaMemset(p->status, 0, sizeof(int)) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_plan_create: memset");
   for (int d = 0; d < 3 && rc == FF_OK; d++) {
-    std::vector<int> ipos(n[d]);
-    for (int q = 0; q < n[d]; q++) ipos[rev[d][q]] = q;
-    if (cudaMemcpy(base + o_rev[d], rev[d].data(), n[d] * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(base + o_ipos[d], ipos.data(), n[d] * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    const int L = len[d];
+    std::vector<int> ipos(L);
+    for (int q = 0; q < L; q++) ipos[rev[d][q]] = q;
+    if (cudaMemcpy(base + o_rev[d], rev[d].data(), L * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(base + o_ipos[d], ipos.data(), L * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
       rc = set_error(FF_ERR_CUDA, "ff_plan_create: table upload failed");
-    const int blocks = std::min(1024, (n[d] + 255) / 256);
-    k_twiddles<<<blocks, 256>>>(n[d], reinterpret_cast<double2 *>(base + o_tw64[d]));
-    if (precision == FF_FP32) k_twiddles<<<blocks, 256>>>(n[d], reinterpret_cast<float2 *>(base + o_tw[d]));
+    const int blocks = std::min(1024, (L + 255) / 256);
+    k_twiddles<<<blocks, 256>>>(L, reinterpret_cast<double2 *>(base + o_tw64[d]));
+    if (precision == FF_FP32) k_twiddles<<<blocks, 256>>>(L, reinterpret_cast<float2 *>(base + o_tw[d]));
     const int cnt = d == 2 ? p->nh : n[d];
     k_wavenumbers<<<std::min(1024, (cnt + 255) / 256), 256>>>(n[d], cnt, d != 2, p->dd[d],
                                                               reinterpret_cast<double *>(base + o_kk[d]));
     p->kk[d] = reinterpret_cast<double *>(base + o_kk[d]);
     AxisDev<double2> ad{};
     AxisDev<float2> af{};
-    ad.n = af.n = n[d];
+    ad.n = af.n = L;
     ad.nstages = af.nstages = (int)radix[d].size();
     for (size_t s = 0; s < radix[d].size(); s++) ad.radix[s] = af.radix[s] = radix[d][s];
     ad.tw = reinterpret_cast<const double2 *>(base + o_tw[d]);
@@ -966,6 +1026,18 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
     ad.ipos = af.ipos = reinterpret_cast<const int *>(base + o_ipos[d]);
     p->axd[d] = ad;
     p->axf[d] = af;
+    if (p->bsM[d] && rc == FF_OK) {
+      const int *drev = reinterpret_cast<const int *>(base + o_rev[d]);
+      if (precision == FF_FP64) {
+        double2 *ch = reinterpret_cast<double2 *>(base + o_chirp[d]), *gh = reinterpret_cast<double2 *>(base + o_ghat[d]);
+        rc = bs_tables<double2>(n[d], L, drev, ch, gh);
+        p->bsd[d] = BsAxis<double2>{ad, n[d], ch, gh};
+      } else {
+        float2 *ch = reinterpret_cast<float2 *>(base + o_chirp[d]), *gh = reinterpret_cast<float2 *>(base + o_ghat[d]);
+        rc = bs_tables<float2>(n[d], L, drev, ch, gh);
+        p->bsf[d] = BsAxis<float2>{af, n[d], ch, gh};
+      }
+    }
   }
   if (rc == FF_OK && cudaGetLastError() != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_plan_create: table kernels");
   if (rc == FF_OK && cudaDeviceSynchronize() != cudaSuccess)

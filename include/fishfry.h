@@ -35,7 +35,8 @@ extern "C" {
 typedef enum {
   FF_OK = 0,
   FF_ERR_INVALID = 1,          /* bad argument (null pointer, non-positive size, ...) */
-  FF_ERR_UNSUPPORTED = 2,      /* length with a prime factor > 5, or above FF_MAX_AXIS */
+  FF_ERR_UNSUPPORTED = 2,      /* length above FF_MAX_AXIS (or, in the batched and serving
+                                  forms, with a prime factor > 5) */
   FF_ERR_BYTES = 3,            /* caller buffers smaller than ff_plan_bytes() */
   FF_ERR_CUDA = 4,             /* a CUDA runtime call failed (message has the name) */
   FF_ERR_NOMEM = 5,            /* device allocation failed */
@@ -72,7 +73,11 @@ typedef struct {
  * dd = 2*pi*(n-1)/(n*(hi-lo)) (ParisPencil.cpp:9-11).  precision is FF_FP64
  * (the plain method) or FF_FP32 (FP32 butterflies, FP64-generated twiddles and
  * 1/k^2).  Allocates the plan's twiddle and index tables on the current device.
- * Each length must be 2^a 3^b 5^c and at most FF_MAX_AXIS. */
+ * Each length must be at most FF_MAX_AXIS.  A length with a prime factor
+ * above 5 (cuFFT, the reference's transform library, takes any length) is
+ * transformed by Bluestein's algorithm through an M-point convolution, M the
+ * smallest 2^a 3^b 5^c >= 2n-1: its passes run plain-load tiles and cost
+ * several times a 2^a 3^b 5^c length's. */
 int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int precision, ff_plan **plan);
 
 /* Bytes each of density and potential must hold (the half spectrum

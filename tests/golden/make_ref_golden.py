@@ -7,7 +7,7 @@ stores f, phi (small grids) or sampled phi values and the phi L2 norm (larger
 grids), plus the relative norms of the reference phi against the analytic
 solution.  It also captures the reference benchmark's own printout.
 
-  python tests/golden/make_ref_golden.py OUTDIR
+  python tests/golden/make_ref_golden.py OUTDIR [NIxNJxNK ...]   (only those grids)
 """
 import os
 import subprocess
@@ -19,8 +19,12 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 REF = os.path.join(ROOT, "oracle", "_ref")
-FULL = [(8, 8, 8), (16, 16, 16), (12, 10, 8), (5, 9, 6), (2, 3, 5), (20, 15, 18)]
-SAMPLED = [(30, 45, 50), (64, 64, 64), (100, 36, 27), (128, 96, 80), (256, 256, 256)]
+# the last two of FULL and of SAMPLED have axes with prime factors above 5
+# (7, 11, 13, 17, 97, 127), which cuFFT transforms and this build runs
+# through its Bluestein passes
+FULL = [(8, 8, 8), (16, 16, 16), (12, 10, 8), (5, 9, 6), (2, 3, 5), (20, 15, 18), (7, 11, 13), (14, 9, 22)]
+SAMPLED = [(30, 45, 50), (64, 64, 64), (100, 36, 27), (128, 96, 80), (256, 256, 256), (97, 60, 49),
+           (127, 34, 64)]
 PRINTOUT = [(8, 8, 8), (16, 16, 16), (64, 64, 64), (128, 128, 128), (256, 256, 256)]
 
 
@@ -40,10 +44,12 @@ def run_dump(n, path):
     return arr[:N].reshape(n), arr[N:].reshape(n), r.stdout.strip()
 
 
-def main(out):
+def main(out, only=None):
     os.makedirs(out, exist_ok=True)
     tmp = os.path.join(out, "_tmp.bin")
     for n in FULL + SAMPLED:
+        if only and n not in only:
+            continue
         f, phi, msg = run_dump(n, tmp)
         name = os.path.join(out, "ref_%dx%dx%d.npz" % n)
         norms = rel_norms(phi)
@@ -57,6 +63,8 @@ def main(out):
         print(name, msg, norms, flush=True)
     os.remove(tmp)
     for n in PRINTOUT:
+        if only and n not in only:
+            continue
         r = subprocess.run([os.path.join(REF, "fishfry_ref"), "1", "1", "1", *map(str, n), "3"], capture_output=True,
                            text=True, timeout=600)
         with open(os.path.join(out, "ref_printout_%dx%dx%d.txt" % n), "w") as fh:
@@ -68,4 +76,5 @@ def main(out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    sel = [tuple(int(x) for x in a.split("x")) for a in sys.argv[2:]]
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"), sel or None)

@@ -37,7 +37,9 @@ def test_version_and_status_strings(ff):
     assert L.ff_plan_phases(None) == 0
 
 
-@pytest.mark.parametrize("n,status", [((7, 8, 8), "FF_ERR_UNSUPPORTED"), ((8, 8, 11), "FF_ERR_UNSUPPORTED"),
+# any length up to FF_MAX_AXIS plans (prime factors above 5 through the
+# Bluestein passes); longer axes and non-positive ones are refused
+@pytest.mark.parametrize("n,status", [((1801, 7, 8), "FF_ERR_UNSUPPORTED"), ((8, 8, 1801), "FF_ERR_UNSUPPORTED"),
                                       ((0, 8, 8), "FF_ERR_INVALID"), ((8, -2, 8), "FF_ERR_INVALID"),
                                       ((8, 8, 2048), "FF_ERR_UNSUPPORTED"), ((8, 8, 1801), "FF_ERR_UNSUPPORTED")])
 def test_plan_rejects_bad_sizes_before_any_device_call(ff, n, status):
