@@ -78,6 +78,14 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zinv(const typename Cplx<T>::t
   }
   __syncthreads();
   const long nlines = (long)a.ni * a.nj;
+  // the same L2 hint as the forward pass, on the spectrum rows (contiguous
+  // for a block's line pairs)
+  if (BULK && threadIdx.x == 32) {
+    const long fl = ((long)blockIdx.x + a.l2_ahead) * (2 * W);
+    if (a.l2_ahead > 0 && fl < nlines)
+      l2_prefetch(spec + fl * a.nhp,
+                  (uint32_t)(min((long)(2 * W), nlines - fl) * a.nhp * sizeof(typename Cplx<T>::type)));
+  }
   const ZTileIO io{&mbar, 0, a.status};
   z_inv_tile<T, N, BULK>(spec, out, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                          reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
@@ -708,11 +716,11 @@ template <typename T> static int configure(ff_plan *p) {
     const int per_plane = fc.prod_pp + fc.cons_pp;
     fc.lag = std::min(ni, std::max(2, (3 * fc.grid + 2 * per_plane - 1) / (2 * per_plane)));
   }
-  // The forward z pass runs one tile per block, three blocks per SM, each
-  // waiting for its inbound line block.  Block b hints block b + l2_ahead's
-  // lines into L2, so that read is under way while the resident blocks
-  // compute and the later bulk copy finds them in L2.  (The same hint on the
-  // strided passes' tensor tiles slowed them.)
+  // The z passes run one tile per block, three blocks per SM, each waiting
+  // for its inbound line block.  Block b hints block b + l2_ahead's lines
+  // (forward) or spectrum rows (inverse) into L2, so that read is under way
+  // while the resident blocks compute and the later bulk copy finds them in
+  // L2.  (The same hint on the strided passes' tensor tiles slowed them.)
   const char *ahead = getenv("FF_L2_AHEAD");
   p->l2_ahead = ahead ? std::max(0, atoi(ahead)) : 3 * p->num_sms;
   const char *mode = getenv("FF_PASSES");

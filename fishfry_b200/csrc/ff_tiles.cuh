@@ -18,7 +18,7 @@ template <typename T> struct PassArgs {
   double invN;             // 1 / (ni*nj*nk)
   double dd[3];            // wavenumber scales (ParisPencil.cpp:9-11)
   int *status;             // device status word (kDev*), 0 = ok
-  int l2_ahead;            // forward z pass: block b prefetches block b + l2_ahead's lines into L2 (0: off)
+  int l2_ahead;            // z passes: block b prefetches block b + l2_ahead's input into L2 (0: off)
 };
 
 constexpr int kZThreads = 256;
