@@ -77,6 +77,11 @@ class Plan:
             return list(times.ms)[:times.count], times.total_ms
         return None
 
+    def solve_passes(self, density, potential, passes, stream=None):
+        """Enqueue only the first `passes` (1..5) passes (ff_solve_passes)."""
+        check(lib().ff_solve_passes(self._h, self.nbytes, _ptr(density), _ptr(potential), _stream(stream),
+                                    int(passes)), "ff_solve_passes")
+
     def phases(self):
         return lib().ff_plan_phases(self._h)
 

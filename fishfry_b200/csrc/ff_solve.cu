@@ -792,7 +792,8 @@ template <typename T> static PassArgs<T> pass_args(const ff_plan *p) {
 }
 
 template <typename T>
-static int launch_solve(const ff_plan *p, void *density, void *potential, cudaStream_t st, bool timed) {
+static int launch_solve(const ff_plan *p, void *density, void *potential, cudaStream_t st, bool timed,
+                        int npass = 5) {
   using C = typename Cplx<T>::type;
   const PassArgs<T> a = pass_args<T>(p);
   T *D = static_cast<T *>(density);
@@ -837,6 +838,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     FF_CUDA(cudaGetLastError());
   }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  if (npass == 1) return FF_OK;
   if (p->bsM[1]) {
     rc = bs_launch<T>(1, Ps, Ps, a, bsax(1), p->bscfg[1], st);
     if (rc != FF_OK) return rc;
@@ -845,6 +847,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     FF_CUDA(cudaGetLastError());
   }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  if (npass == 2) return FF_OK;
   if (p->bsM[0]) {
     rc = bs_launch<T>(2, Ps, Ps, a, bsax(0), p->bscfg[2], st);
     if (rc != FF_OK) return rc;
@@ -853,6 +856,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     FF_CUDA(cudaGetLastError());
   }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  if (npass == 3) return FF_OK;
   if (p->bsM[1]) {
     rc = bs_launch<T>(3, Ps, Ds, a, bsax(1), p->bscfg[3], st);
     if (rc != FF_OK) return rc;
@@ -861,6 +865,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     FF_CUDA(cudaGetLastError());
   }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
+  if (npass == 4) return FF_OK;
   if (p->bsM[2]) {
     rc = bs_launch<T>(4, Ds, P, a, bsax(2), p->bscfg[4], st);
     if (rc != FF_OK) return rc;
@@ -1100,6 +1105,19 @@ int ff_solve(const ff_plan *p, size_t bytes, void *density, void *potential, voi
     return take_device_status(p, st);
   }
   return FF_OK;
+}
+
+int ff_solve_passes(const ff_plan *p, size_t bytes, void *density, void *potential, void *stream, int passes) {
+  if (!p || !density || !potential) return set_error(FF_ERR_INVALID, "ff_solve_passes: null argument");
+  if (passes < 1 || passes > 5) return set_error(FF_ERR_INVALID, "ff_solve_passes: passes = %d", passes);
+  if (p->fused) return set_error(FF_ERR_INVALID, "ff_solve_passes: the plan fuses its passes (FF_PASSES=3)");
+  if (bytes < p->bytes) return set_error(FF_ERR_BYTES, "ff_solve_passes: bytes %zu < required %zu", bytes, p->bytes);
+  if (density == potential) return set_error(FF_ERR_INVALID, "ff_solve_passes: density and potential must differ");
+  if (((uintptr_t)density | (uintptr_t)potential) & 15)
+    return set_error(FF_ERR_INVALID, "ff_solve_passes: buffers must be 16-byte aligned");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->precision == FF_FP64 ? launch_solve<double>(p, density, potential, st, false, passes)
+                                 : launch_solve<float>(p, density, potential, st, false, passes);
 }
 
 int ff_plan_check(const ff_plan *p, void *stream) {

@@ -103,6 +103,19 @@ const char *ff_phase_name(const ff_plan *plan, int q);
 int ff_solve(const ff_plan *plan, size_t bytes, void *density, void *potential, void *stream,
              ff_phase_times *times);
 
+/* Diagnostic: enqueues only the first `passes` (1..5) of ff_solve's five
+ * passes, so each pass can be checked on its own; every intermediate is in
+ * natural order.  After pass 1 potential holds the half spectrum along z,
+ * S[i][j][kh] (kh < n2/2+1, row pitch: n2/2+1 complex values FP64, that
+ * rounded up to even FP32); after pass 2 that spectrum transformed along y
+ * (unnormalised forward DFT); after pass 3 transformed along x, multiplied by
+ * the filter -1/(k^2 N) (0 at the zero mode) and transformed back along x
+ * (unnormalised inverse DFT); after pass 4 density holds it transformed back
+ * along y; pass 5 completes the solve (potential = phi).  No counterpart in
+ * the reference, whose phase stamps (ParisPencil.cpp:142-424) time the same
+ * steps.  FF_ERR_INVALID for a plan whose passes are fused (FF_PASSES=3). */
+int ff_solve_passes(const ff_plan *plan, size_t bytes, void *density, void *potential, void *stream, int passes);
+
 /* Reads and clears the plan's device status word (waits for `stream`).
  * Returns FF_ERR_TIMEOUT if a bounded wait inside a solve kernel gave up since
  * the last check (a TMA tile copy that never completed); that solve's result
