@@ -1,5 +1,5 @@
 // Bluestein passes of the single-grid solve for axes with a prime factor
-// above 5 (the algorithm and its tables are described in ff_bluestein.hpp).
+// above 7 (the algorithm and its tables are described in ff_bluestein.hpp).
 //
 // One kernel per pass kind, runtime plans only (M varies with n):
 //   z forward / inverse: W line pairs per block in a line-major swizzled tile
@@ -66,7 +66,7 @@ template <bool INV, Map MAP, int W, bool TWREC0, typename C, typename LD0, typen
 __device__ __forceinline__ void bs_core(const BsAxis<C> &bs, LD0 &ld0, TILE &tile, STL &stl, int ncols) {
   constexpr bool TWALL = sizeof(C) == 16;   // FP64: recurrence twiddles in every stage
   const AxisDev<C> &ax = bs.m;
-  const int S = ax.nstages;   // M >= 13, so at least two stages
+  const int S = ax.nstages;   // n >= 11, so M >= 21: at least two stages
   dif_rt<false, MAP, W, kBsThreads, TWREC0, TWALL>(ax, S - 1, ld0, tile, tile, ncols);
   with_radix(ax.radix[S - 1], [&](auto tag) {
     constexpr int R = decltype(tag)::value;
@@ -275,7 +275,7 @@ template <typename F> int raise_smem(F fn, size_t need) {
 
 int bs_padded_length(int n) {
   for (int m = std::max(1, 2 * n - 1);; m++)
-    if (smooth235(m)) return m;
+    if (smooth2357(m)) return m;
 }
 
 template <typename T> int bs_configure(int kind, int ni, int nj, int nh, int M, BsCfg *cfg) {

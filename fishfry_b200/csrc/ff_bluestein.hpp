@@ -1,12 +1,12 @@
-// Axes whose length has a prime factor above 5 (single-grid solve).
+// Axes whose length has a prime factor above 7 (single-grid solve).
 //
 // cuFFT, which the reference calls for every line transform
 // (ParisPencil.cpp:78-81 plans, :165/:212/:259/:288/:334/:380 executions),
-// accepts any length.  Here an axis of n points with a prime factor above 5
+// accepts any length.  Here an axis of n points with a prime factor above 7
 // is transformed by Bluestein's algorithm: with the chirp
 // c[j] = exp(-i*pi*j^2/n), the forward DFT is
 //   X[k] = c[k] * sum_j (x[j] c[j]) conj c[k-j],
-// a circular convolution of M >= 2n-1 points (M = 2^a 3^b 5^c), computed by
+// a circular convolution of M >= 2n-1 points (M = 2^a 3^b 5^c 7^d), computed by
 // the same mixed-radix stages as every other axis: an M-point forward DIF
 // transform of the premultiplied, zero-padded line, a product with the
 // transform of the convolution kernel (one register group, with the last DIF
@@ -32,7 +32,7 @@ template <typename C> struct BsAxis {
                      // G the M-point DFT of g[m] = conj chirp[|m|] (|m| < n, indices mod M)
 };
 
-// Smallest 2^a 3^b 5^c >= 2n - 1.
+// Smallest 2^a 3^b 5^c 7^d >= 2n - 1.
 int bs_padded_length(int n);
 
 // Launch shape of one Bluestein pass.

@@ -65,6 +65,13 @@ template <> struct Real<float2> { using type = float; };
 #define FF_C5_2 (-0.80901699437494742410229341718281905886)
 #define FF_S5_1 0.95105651629515357211643933337938214340
 #define FF_S5_2 0.58778525229247312916870595463907276860
+// cos and sin of 2*pi*k/7, k = 1, 2, 3
+#define FF_C7_1 0.62348980185873353052500488400423981063
+#define FF_C7_2 (-0.22252093395631440428890256449679475947)
+#define FF_C7_3 (-0.90096886790241912623610231950744505117)
+#define FF_S7_1 0.78183148246802980870844452667405775023
+#define FF_S7_2 0.97492791218182360701813168299393121723
+#define FF_S7_3 0.43388373911755812047576833284835875461
 
 // In-register R-point DFT, y_s = sum_r v_r exp(-+2*pi*i*r*s/R), unnormalised.
 template <int R, bool INV, typename C> struct Dft;
@@ -124,6 +131,36 @@ template <bool INV, typename C> struct Dft<5, INV, C> {
   }
 };
 
+// 7 points: with t_k = v_k + v_{7-k} and u_k = v_k - v_{7-k} (k = 1..3),
+// y_m = v_0 + sum_k cos(2*pi*k*m/7) t_k -+ i sum_k sin(2*pi*k*m/7) u_k and
+// y_{7-m} the same with the sign of the sine sum flipped (m = 1..3).
+template <bool INV, typename C> struct Dft<7, INV, C> {
+  static __device__ __forceinline__ void run(C *v) {
+    using T = typename Real<C>::type;
+    const C t1 = cadd(v[1], v[6]), t2 = cadd(v[2], v[5]), t3 = cadd(v[3], v[4]);
+    const C u1 = csub(v[1], v[6]), u2 = csub(v[2], v[5]), u3 = csub(v[3], v[4]);
+    const C a0 = v[0];
+    const T c1 = (T)FF_C7_1, c2 = (T)FF_C7_2, c3 = (T)FF_C7_3;
+    const T s1 = (T)FF_S7_1, s2 = (T)FF_S7_2, s3 = (T)FF_S7_3;
+    // cosine sums (k*m mod 7 folded to 1..3)
+    const C b1 = mk(a0.x + c1 * t1.x + c2 * t2.x + c3 * t3.x, a0.y + c1 * t1.y + c2 * t2.y + c3 * t3.y);
+    const C b2 = mk(a0.x + c2 * t1.x + c3 * t2.x + c1 * t3.x, a0.y + c2 * t1.y + c3 * t2.y + c1 * t3.y);
+    const C b3 = mk(a0.x + c3 * t1.x + c1 * t2.x + c2 * t3.x, a0.y + c3 * t1.y + c1 * t2.y + c2 * t3.y);
+    // sine sums: sin(2*pi*j/7) = -sin(2*pi*(7-j)/7) for j > 3
+    const C d1 = mk(s1 * u1.x + s2 * u2.x + s3 * u3.x, s1 * u1.y + s2 * u2.y + s3 * u3.y);
+    const C d2 = mk(s2 * u1.x - s3 * u2.x - s1 * u3.x, s2 * u1.y - s3 * u2.y - s1 * u3.y);
+    const C d3 = mk(s3 * u1.x - s1 * u2.x + s2 * u3.x, s3 * u1.y - s1 * u2.y + s2 * u3.y);
+    v[0] = cadd(a0, cadd(t1, cadd(t2, t3)));
+    const C e1 = mul_wi<INV>(d1), e2 = mul_wi<INV>(d2), e3 = mul_wi<INV>(d3);   // -i*d forward
+    v[1] = cadd(b1, e1);
+    v[6] = csub(b1, e1);
+    v[2] = cadd(b2, e2);
+    v[5] = csub(b2, e2);
+    v[3] = cadd(b3, e3);
+    v[4] = csub(b3, e3);
+  }
+};
+
 template <bool INV, typename C> struct Dft<8, INV, C> {
   static __device__ __forceinline__ void run(C *v) {
     using T = typename Real<C>::type;
@@ -156,15 +193,16 @@ template <bool INV, typename C> struct Dft<8, INV, C> {
 };
 
 // ------------------------------------------------------------ radix plan
-// Radix order of a DIF transform of length n = 2^a 3^b 5^c: radix 8 while
-// three factors of 2 remain, then one 4 or 2, then the 5s, then the 3s; a
-// length of 1 is one stage of radix 1.  Shared by host planning and device
-// code, so compile-time specialised kernels and plan tables agree.
+// Radix order of a DIF transform of length n = 2^a 3^b 5^c 7^d: radix 8
+// while three factors of 2 remain, then one 4 or 2, then the 5s, the 3s and
+// the 7s; a length of 1 is one stage of radix 1.  Shared by host planning and
+// device code, so compile-time specialised kernels and plan tables agree.
 __host__ __device__ constexpr int plan_radix(int n, int s) {
-  int twos = 0, fives = 0, threes = 0, m = n;
+  int twos = 0, fives = 0, threes = 0, sevens = 0, m = n;
   while (m > 1 && m % 2 == 0) { m /= 2; twos++; }
   while (m > 1 && m % 5 == 0) { m /= 5; fives++; }
   while (m > 1 && m % 3 == 0) { m /= 3; threes++; }
+  while (m > 1 && m % 7 == 0) { m /= 7; sevens++; }
   const int eights = twos / 3, rest = twos % 3;
   if (s < eights) return 8;
   s -= eights;
@@ -175,13 +213,15 @@ __host__ __device__ constexpr int plan_radix(int n, int s) {
   if (s < fives) return 5;
   s -= fives;
   if (s < threes) return 3;
+  s -= threes;
+  if (s < sevens) return 7;
   return 1;
 }
 __host__ __device__ constexpr int plan_stages(int n) {
   int s = 0;
   for (int q = 0, L = n; L > 1; q++) {
     const int r = plan_radix(n, q);
-    if (r == 1) break;   // n is not 2^a 3^b 5^c
+    if (r == 1) break;   // n is not 2^a 3^b 5^c 7^d
     L /= r;
     s++;
   }
@@ -375,6 +415,7 @@ template <typename F> __device__ __forceinline__ void with_radix(int r, F &&f) {
     case 2: f(RadixTag<2>{}); break;
     case 5: f(RadixTag<5>{}); break;
     case 3: f(RadixTag<3>{}); break;
+    case 7: f(RadixTag<7>{}); break;
     default: f(RadixTag<1>{}); break;
   }
 }

@@ -489,8 +489,8 @@ struct ff_plan {
   int l2_ahead;        // forward z pass: L2 prefetch distance in blocks (0: off)
   StridedCfg ycfg, xcfg;
   FusedCfg fwd, inv;
-  // axes with a prime factor above 5: padded convolution length M (0 for a
-  // 2^a 3^b 5^c axis), their tables, and the launch shape of each pass kind
+  // axes with a prime factor above 7: padded convolution length M (0 for a
+  // 2^a 3^b 5^c 7^d axis), their tables, and the launch shape of each pass kind
   // (0 z fwd, 1 y fwd, 2 x, 3 y inv, 4 z inv) that transforms such an axis
   int bsM[3];
   BsAxis<double2> bsd[3];
@@ -504,6 +504,13 @@ namespace ff {
 bool smooth235(int n) {
   if (n < 1) return false;
   for (int p : {2, 3, 5})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+bool smooth2357(int n) {
+  if (n < 1) return false;
+  for (int p : {2, 3, 5, 7})
     while (n % p == 0) n /= p;
   return n == 1;
 }
@@ -638,7 +645,7 @@ template <typename T> static int configure(ff_plan *p) {
   const size_t csz = sizeof(C);
   const int ni = p->n[0], nj = p->n[1], nk = p->n[2];
   int rc = FF_OK;
-  // passes along an axis with a prime factor above 5 (pass kind -> axis)
+  // passes along an axis with a prime factor above 7 (pass kind -> axis)
   const int axis_of_kind[5] = {2, 1, 0, 1, 2};
   for (int kind = 0; kind < 5 && rc == FF_OK; kind++)
     if (p->bsM[axis_of_kind[kind]])
@@ -975,7 +982,7 @@ int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int p
   size_t o_tw[3], o_tw64[3], o_rev[3], o_ipos[3], o_kk[3], o_chirp[3] = {0, 0, 0}, o_ghat[3] = {0, 0, 0};
   auto take = [&](size_t b) { size_t o = off; off += (b + 255) & ~size_t(255); return o; };
   for (int d = 0; d < 3; d++) {
-    p->bsM[d] = smooth235(n[d]) ? 0 : bs_padded_length(n[d]);
+    p->bsM[d] = smooth2357(n[d]) ? 0 : bs_padded_length(n[d]);
     const int L = len[d] = p->bsM[d] ? p->bsM[d] : n[d];
     radix[d] = plan_factor_radices(L);
     if ((int)radix[d].size() > kMaxStages) {

@@ -25,5 +25,7 @@ int set_error(int status, const char *fmt, ...);
 
 // Axis length check: 1..FF_MAX_AXIS with prime factors 2, 3, 5 only.
 bool smooth235(int n);
+// Prime factors 2, 3, 5 and 7 only (the radices of the single-grid plans).
+bool smooth2357(int n);
 
 }  // namespace ff

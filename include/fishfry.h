@@ -74,10 +74,11 @@ typedef struct {
  * (the plain method) or FF_FP32 (FP32 butterflies, FP64-generated twiddles and
  * 1/k^2).  Allocates the plan's twiddle and index tables on the current device.
  * Each length must be at most FF_MAX_AXIS.  A length with a prime factor
- * above 5 (cuFFT, the reference's transform library, takes any length) is
+ * above 7 (cuFFT, the reference's transform library, takes any length) is
  * transformed by Bluestein's algorithm through an M-point convolution, M the
- * smallest 2^a 3^b 5^c >= 2n-1: its passes run plain-load tiles and cost
- * several times a 2^a 3^b 5^c length's. */
+ * smallest 2^a 3^b 5^c 7^d >= 2n-1: its passes run plain-load tiles and
+ * cost several times a 2^a 3^b 5^c 7^d length's (radix 8, 4, 2, 5, 3 and 7
+ * stages). */
 int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int precision, ff_plan **plan);
 
 /* Bytes each of density and potential must hold (the half spectrum

@@ -1,9 +1,10 @@
-"""GPU tests of axes whose length has a prime factor above 5.
+"""GPU tests of axes whose length has a prime factor of 7 or above.
 
-cuFFT, which the reference calls for its line transforms, accepts any length;
-here such an axis runs through the Bluestein passes (an M-point circular
-convolution, M = 2^a 3^b 5^c >= 2n - 1).  Checked against the CPU oracle
-(its FFT takes every length: a direct DFT for prime factors above 5), against
+cuFFT, which the reference calls for its line transforms, accepts any length.
+Here factors of 7 run direct radix-7 stages, and an axis with a prime factor
+above 7 runs through the Bluestein passes (an M-point circular convolution,
+M = 2^a 3^b 5^c 7^d >= 2n - 1).  Checked against the CPU oracle (its FFT
+takes every length: a direct DFT for prime factors above 5), against
 golden vectors the reference itself wrote on a B200 (tests/golden/), and
 against exact single-mode solutions.
 
@@ -45,7 +46,7 @@ def solve(torch, ff, f, precision=0, lo=None, hi=None):
     return p[:f.size].double().cpu().numpy().reshape(n)
 
 
-# prime factors above 5 on one, two or three axes, with compile-time (64,
+# prime factors of 7 and above on one, two or three axes, with compile-time (64,
 # 128, 256, 512), runtime and one-point axes beside them, and the largest
 # padded length (1789 -> M = 3600)
 SIZES = [(7, 8, 8), (8, 8, 11), (7, 11, 13), (14, 9, 22), (33, 34, 35), (127, 64, 64), (64, 127, 64),
@@ -62,6 +63,21 @@ def test_fp64_parity_with_oracle(torch_cuda, ff, oracle, n):
     assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL, n
 
 
+# 2^a 3^b 5^c 7^d axes (direct radix-7 stages), up to 1792 = 2^8 * 7 points
+RADIX7 = [(448, 7, 12), (14, 343, 8), (28, 49, 196), (1792, 2, 4), (6, 5, 1792), (21, 35, 63), (112, 224, 56)]
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, FP32_TOL)])
+@pytest.mark.parametrize("n", RADIX7)
+def test_radix7_axes_match_oracle(torch_cuda, ff, oracle, n, precision, tol):
+    rng = np.random.default_rng(7 * sum(n) + precision)
+    f = rng.standard_normal(n)
+    if precision:
+        f = f.astype(np.float32).astype(np.float64)
+    phi = solve(torch_cuda, ff, f, precision=precision)
+    assert rel_l2(phi, oracle.solve(f)) <= tol, n
+
+
 @pytest.mark.parametrize("n", [(7, 11, 13), (97, 60, 49), (64, 127, 64), (4, 1789, 3), (33, 34, 35)])
 def test_fp32_parity_with_oracle(torch_cuda, ff, oracle, n):
     rng = np.random.default_rng(3 * sum(n))
@@ -73,7 +89,9 @@ def test_fp32_parity_with_oracle(torch_cuda, ff, oracle, n):
 @pytest.mark.parametrize("n", [(31, 37, 41), (127, 64, 49), (17, 19, 23)])
 def test_reference_field_norms_match_oracle(torch_cuda, ff, oracle, n):
     """The reference's analytic f (FishFry.hpp:22-44) and its error norms on
-    grids of prime lengths: device norms equal the oracle's."""
+    grids of prime lengths: device norms equal the oracle's where the grid's
+    truncation error sets them (17x19x23: 2e-8), and both are round-off
+    (about 1e-15, where the two solves' rounding differs) on the finer grids."""
     plan = ff.Plan(n)
     d = torch_cuda.empty(plan.nbytes // 8, dtype=torch_cuda.float64, device="cuda")
     p = torch_cuda.empty_like(d)
@@ -85,7 +103,7 @@ def test_reference_field_norms_match_oracle(torch_cuda, ff, oracle, n):
     assert rel_l2(p[:N].cpu().numpy().reshape(n), ref) <= FP64_TOL
     got = ff.rel_norms(n, p)
     want = oracle.rel_norms(ref)
-    assert all(abs(a - b) <= 1e-12 * max(b, 1e-300) + 1e-15 for a, b in zip(got, want)), (got, want)
+    assert all(abs(a - b) <= 1e-9 * b + 5e-15 for a, b in zip(got, want)), (got, want)
 
 
 @pytest.mark.parametrize("n,L", [((7, 11, 13), (1.0, 2.0, 3.0)), ((97, 16, 49), (5.0, 0.5, 2.0))])
