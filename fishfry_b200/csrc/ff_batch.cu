@@ -196,7 +196,7 @@ std::vector<int> batch_radix_order(int n, int order) {
   if (order == 1) {
     std::reverse(r.begin(), r.end());
   } else if (order == 2) {
-    std::stable_partition(r.begin(), r.end(), [](int x) { return x == 5 || x == 3; });
+    std::stable_partition(r.begin(), r.end(), [](int x) { return x == 5 || x == 3 || x == 7; });
   } else if (order != 0) {
     return {};
   }
@@ -281,9 +281,9 @@ size_t batch_grid_bytes(const BatchGridHost &h, int precision) {
 int batch_check_dims(const int n[3], const double *lo, const double *hi, const char *who, int g) {
   for (int d = 0; d < 3; d++) {
     if (n[d] < 1) return set_error(FF_ERR_INVALID, "%s: grid %d n[%d] = %d < 1", who, g, d, n[d]);
-    if (n[d] > FF_MAX_AXIS || !smooth235(n[d]))
-      return set_error(FF_ERR_UNSUPPORTED, "%s: grid %d n[%d] = %d is not 2^a 3^b 5^c <= %d", who, g, d, n[d],
-                       FF_MAX_AXIS);
+    if (n[d] > FF_MAX_AXIS || !smooth2357(n[d]))
+      return set_error(FF_ERR_UNSUPPORTED, "%s: grid %d n[%d] = %d is not 2^a 3^b 5^c 7^d <= %d", who, g, d,
+                       n[d], FF_MAX_AXIS);
     if (lo && hi && n[d] > 1 && !(hi[d] > lo[d]))
       return set_error(FF_ERR_INVALID, "%s: grid %d hi[%d] <= lo[%d]", who, g, d, d);
     // the narrowest tile of a strided pass holds whole lines of 128-byte rows

@@ -23,9 +23,9 @@ int set_error(int status, const char *fmt, ...);
                              __LINE__, cudaGetErrorName(e_), cudaGetErrorString(e_));       \
   } while (0)
 
-// Axis length check: 1..FF_MAX_AXIS with prime factors 2, 3, 5 only.
+// Prime factors 2, 3, 5 only.
 bool smooth235(int n);
-// Prime factors 2, 3, 5 and 7 only (the radices of the single-grid plans).
+// Prime factors 2, 3, 5 and 7 only (the radices of the FFT stages).
 bool smooth2357(int n);
 
 }  // namespace ff

@@ -36,7 +36,7 @@ typedef enum {
   FF_OK = 0,
   FF_ERR_INVALID = 1,          /* bad argument (null pointer, non-positive size, ...) */
   FF_ERR_UNSUPPORTED = 2,      /* length above FF_MAX_AXIS (or, in the batched and serving
-                                  forms, with a prime factor > 5) */
+                                  forms, with a prime factor > 7) */
   FF_ERR_BYTES = 3,            /* caller buffers smaller than ff_plan_bytes() */
   FF_ERR_CUDA = 4,             /* a CUDA runtime call failed (message has the name) */
   FF_ERR_NOMEM = 5,            /* device allocation failed */
@@ -127,7 +127,7 @@ int ff_plan_destroy(ff_plan *plan);
 
 /* ---- Batched form (no counterpart in the reference, which solves one grid
  * per ParisPencil).  `count` independent grids, dims[3g..3g+2] = (ni, nj, nk)
- * of grid g, each axis 2^a 3^b 5^c and at most 574 points; lo/hi (3 per grid)
+ * of grid g, each axis 2^a 3^b 5^c 7^d and at most 574 points; lo/hi (3 per grid)
  * give the physical bounds as ParisPencil's constructor takes them
  * (ParisPencil.hpp:23), or NULL for the reference's domain [-pi, pi - 2pi/n].
  * A solve of the batch runs the same five passes as ff_solve, each pass one

@@ -95,7 +95,7 @@ def test_driver_arguments_checked_on_host(ff):
     assert r.returncode == 1
 
 
-@pytest.mark.parametrize("dims,status", [([], "FF_ERR_INVALID"), ([(8, 8, 7)], "FF_ERR_UNSUPPORTED"),
+@pytest.mark.parametrize("dims,status", [([], "FF_ERR_INVALID"), ([(8, 8, 11)], "FF_ERR_UNSUPPORTED"),
                                          ([(8, 8, 8), (0, 4, 4)], "FF_ERR_INVALID"),
                                          ([(576, 8, 8)], "FF_ERR_UNSUPPORTED"), ([(8, 11, 8)], "FF_ERR_UNSUPPORTED")])
 def test_batch_rejects_bad_dims_before_any_device_call(ff, dims, status):

@@ -153,9 +153,46 @@ def test_matches_reference_golden(torch_cuda, ff, path):
         assert abs(np.linalg.norm(phi) - float(g["phi_l2"])) <= FP64_TOL * float(g["phi_l2"])
 
 
-def test_batch_still_rejects_prime_lengths(ff):
-    """The batched and serving forms keep 2^a 3^b 5^c lengths (their tiles
-    hold whole lines); the single-grid plan takes any length."""
+def test_batch_rejects_primes_above_7(ff):
+    """The batched and serving forms take 2^a 3^b 5^c 7^d lengths (no
+    Bluestein passes there); the single-grid plan takes any length."""
     with pytest.raises(ff.FFError) as e:
-        ff.Batch([(8, 8, 7)])
+        ff.Batch([(8, 8, 11)])
     assert e.value.status == ff.FF_ERR_UNSUPPORTED
+
+
+def test_batch_and_server_radix7_lengths(torch_cuda, ff, oracle):
+    """2^a 3^b 5^c 7^d grids in a batch (default and tuned shapes) and through
+    the server, FP64 and FP32, against the oracle."""
+    dims = [(28, 49, 56), (112, 14, 21), (7, 8, 8), (35, 63, 98), (64, 7, 343)]
+    for prec, tol in ((0, FP64_TOL), (1, FP32_TOL)):
+        batch = ff.Batch(dims, precision=prec)
+        dt = torch_cuda.float64 if prec == 0 else torch_cuda.float32
+        esz = 8 if prec == 0 else 4
+        d = [torch_cuda.zeros(nb // esz, dtype=dt, device="cuda") for nb in batch.nbytes]
+        p = [torch_cuda.empty_like(x) for x in d]
+        rng = np.random.default_rng(77 + prec)
+        fs = [rng.standard_normal(n).astype(np.float32).astype(np.float64) for n in dims]
+        for tuned in (False, True):
+            for g, f in enumerate(fs):
+                d[g][:f.size] = torch_cuda.from_numpy(f.ravel()).to(dt).cuda()
+            if tuned:
+                batch.tune(d, p, reps=1)
+                for g, f in enumerate(fs):
+                    d[g][:f.size] = torch_cuda.from_numpy(f.ravel()).to(dt).cuda()
+            batch.solve(d, p)
+            for g, f in enumerate(fs):
+                phi = p[g][:f.size].double().cpu().numpy().reshape(dims[g])
+                assert rel_l2(phi, oracle.solve(f)) <= tol, (prec, tuned, dims[g])
+    srv = ff.Server(1 << 30, max_active=8)
+    try:
+        for q, n in enumerate(dims[:3]):
+            f = torch_cuda.from_numpy(np.random.default_rng(q).standard_normal(n).ravel()).cuda()
+            rid = srv.submit(n, f, 0)
+            srv.wait(rid)
+            out = torch_cuda.empty_like(f)
+            srv.fetch(rid, out)
+            ref = oracle.solve(f.cpu().numpy().reshape(n))
+            assert rel_l2(out.cpu().numpy().reshape(n), ref) <= FP64_TOL, n
+    finally:
+        srv.close()
