@@ -25,7 +25,9 @@ def numpy_solve(f, dd=(1.0, 1.0, 1.0)):
     return np.fft.irfftn(F, s=f.shape, axes=(0, 1, 2))
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 8, 9, 12, 15, 16, 25, 27, 30, 45, 64, 97, 120, 125, 243, 512, 1000])
+# 2^a 3^b 5^c, 7-smooth (49, 343, 448, 1792) and prime (11, 13, 97, 127, 1789) lengths
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 6, 7, 8, 9, 11, 12, 13, 15, 16, 25, 27, 30, 45, 49, 64, 97, 120, 125, 127,
+                               243, 343, 448, 512, 1000, 1789, 1792])
 def test_fft1d_matches_numpy(oracle, n):
     rng = np.random.default_rng(n)
     x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
@@ -36,7 +38,7 @@ def test_fft1d_matches_numpy(oracle, n):
 
 
 @pytest.mark.parametrize("n", [(8, 8, 8), (16, 16, 16), (12, 10, 8), (5, 9, 6), (30, 45, 50), (7, 5, 9),
-                               (1, 4, 6), (3, 1, 1), (2, 3, 5), (64, 48, 40)])
+                               (1, 4, 6), (3, 1, 1), (2, 3, 5), (64, 48, 40), (7, 11, 13), (14, 9, 22), (49, 33, 17)])
 def test_solve_matches_numpy(oracle, n):
     rng = np.random.default_rng(sum(n))
     f = rng.standard_normal(n)
