@@ -15,6 +15,20 @@ Under torchrun (N > 1) every rank solves its own grid (replicas, weak
 scaling: the single-grid solve has no exchange step on one GPU); the time is
 the max over ranks.
 
+The default line also carries the other two parts of the headline metric,
+each measured in the same run with its own clock record and error figures
+(skipped with --no-extras, and under torchrun):
+  batch      256 seeded grids, dims iid {32..128}: FP32 and FP64 batched
+             solves/s against a loop of plain FP64 solves of the same grids,
+             max relative L2 against those plain FP64 solves;
+  serve      Poisson request streams (dims 5-smooth in [32, 512], log-uniform
+             points): p50/p99 at 1000 requests/s with FP32:FP64 1:1, solves/s
+             at saturation for the 1:1 mix and for FP32 alone, against plain
+             FP64 and FP32 loops over the same requests; FP32 error against
+             the plain FP64 solve;
+  precision  1024^3 FP32 (FP64 twiddles and 1/k^2) with 64 seeded modes:
+             points/s and relative L2/Linf against the FP64 solve of the same f.
+
 --impl reference times the reference algorithm on the host cores: the
 reference has no CPU code path, so this is the oracle's OpenMP restatement
 (oracle/), on all host threads; rank 0 only.
@@ -63,6 +77,8 @@ def parse():
     ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM admission budget")
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--no-tune", action="store_true", help="batch: default tile shapes, no autotuning")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line without the batch, serve and precision keys")
     return ap.parse_args()
 
 
@@ -241,6 +257,15 @@ def scipy_yardstick(n, threads):
     return dt, f.size / dt
 
 
+def solve_config(n, precision, world):
+    """The `config` of the solve workload, identical in both arms."""
+    esz = 8 if precision == "fp64" else 4
+    N = n[0] * n[1] * n[2]
+    return {"workload": "%dx%dx%d %s Poisson solve" % (*n, precision.upper()), "grid": list(n),
+            "precision": precision, "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (%.2f GB per field > 126 MB)" % (N * esz / 1e9)}
+
+
 def run_reference(args):
     """The reference's algorithm on the host cores: each step one oracle
     solve (ParisPencil's FFT solve restated in C++/OpenMP) of a sample grid
@@ -258,8 +283,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: analytic f of FishFry.hpp:22-44 on the reference grid",
-        "config": {"workload": "%dx%dx%d FP64 Poisson solve" % tuple(args.grid), "grid": list(args.grid),
-                   "precision": "fp64", "parallelism": "host threads", "sample_grid": list(sample)},
+        "config": solve_config(tuple(args.grid), "fp64", args.gpus),
+        "sample_grid": list(sample),
         "cpu_baseline": {"value": value, "unit": "points/s", "cores": cores, "kind": "port",
                          "sample": "%d solves of a %dx%dx%d sample grid on %s" % (args.steps, *sample,
                                                                                 cpu_info() or "host")},
@@ -434,10 +459,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == ff.FF_FP64 else "f32",
             "data": "synthetic: analytic f of FishFry.hpp:22-44 on the reference grid (x = -pi + i*2*pi/n)",
-            "config": {"workload": "%dx%dx%d %s Poisson solve, 5 passes" % (*n, args.precision.upper()),
-                       "grid": list(n), "precision": args.precision,
-                       "parallelism": "replicas x%d" % world if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (%.2f GB per field > 126 MB)" % (N * esz / 1e9)},
+            "config": solve_config(n, args.precision, world),
             "roofline": {"bound": "hbm", "kernel": names[top], "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                          "algorithmic_bytes": per_pass_bytes[top]},
@@ -452,8 +474,23 @@ def run_ours(args):
             "clocks": clk,
             "check": {"rel_l1_l2_linf_vs_analytic": norms},
         }
-        print(json.dumps(line), flush=True)
     plan.close()
+    del d, p, f0
+    if e2e is not None:
+        del dd, pp, hf, hp, ref
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the other parts of the headline metric, each with its own clocks
+        for key, fn in (("batch", extra_batch), ("serve", extra_serve), ("precision", extra_precision)):
+            t = time.perf_counter()
+            try:
+                line[key] = fn(args)
+            except Exception as e:   # an extra that fails does not cost the headline line
+                line[key] = {"error": "%s: %s" % (type(e).__name__, str(e)[:300])}
+            line[key]["wall_s"] = time.perf_counter() - t
+            torch.cuda.empty_cache()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
@@ -470,18 +507,19 @@ def rel_l2_dev(torch, a, b):
     return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
 
 
-def run_precision(args):
-    """1024^3 FP32 solve of analytic f + 64 seeded modes; error against the
-    FP64 solve of the same input and against the analytic potential."""
+def precision_measure(n, steps, warmup, seed):
+    """FP64 and FP32 solves of grid n, f = analytic + 64 seeded modes: ms per
+    solve (CUDA events), and the FP32 error against the FP64 solve of the
+    same f and against the analytic potential, all computed on the device."""
     import torch
 
     import fishfry_b200 as ff
-    n = tuple(args.grid) if args.grid != [512, 512, 512] else (1024, 1024, 1024)
     N = n[0] * n[1] * n[2]
-    modes = modes_for(ff, n, args.seed)
+    modes = modes_for(ff, n, seed)
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(device=dev)
     res = {}
+    clocks = ClockSampler(0)
     for prec in (ff.FF_FP64, ff.FF_FP32):
         dt = torch.float64 if prec == ff.FF_FP64 else torch.float32
         plan = ff.Plan(n, precision=prec)
@@ -491,31 +529,53 @@ def run_precision(args):
         f0 = torch.empty(N, dtype=dt, device=dev)
         ff.init_field(n, f0, modes, prec)
         times = []
-        for it in range(max(args.warmup, 3) + args.steps):
-            d[:N].copy_(f0)
-            torch.cuda.synchronize()
+        for it in range(max(warmup, 3) + steps):
+            if it == max(warmup, 3) and prec == ff.FF_FP32:
+                clocks.start()
+            with torch.cuda.stream(stream):
+                d[:N].copy_(f0)
             ms, tot = plan.solve(d, p, stream=stream, timed=True)
-            if it >= max(args.warmup, 3):
+            if it >= max(warmup, 3):
                 times.append(tot)
         res[prec] = {"ms": sum(times) / len(times), "phi": p[:N].clone(),
                      "norms": ff.rel_norms(n, p, modes, prec)}
         plan.close()
         del d, p, f0
         torch.cuda.empty_cache()
+    clk = clocks.stop()
     p64, p32 = res[ff.FF_FP64]["phi"], res[ff.FF_FP32]["phi"]
     diff = (p32.double() - p64)
+    out = {"grid": list(n), "fp32_ms_per_solve": res[ff.FF_FP32]["ms"], "fp64_ms_per_solve": res[ff.FF_FP64]["ms"],
+           "fp32_points_per_s": N / (res[ff.FF_FP32]["ms"] * 1e-3),
+           "fp64_points_per_s": N / (res[ff.FF_FP64]["ms"] * 1e-3),
+           "fp32_vs_fp64_solve": {"rel_l2": rel_l2_dev(torch, p32, p64),
+                                  "rel_linf": float(diff.abs().max() / p64.abs().max())},
+           "fp32_vs_analytic_rel_l1_l2_linf": res[ff.FF_FP32]["norms"],
+           "fp64_vs_analytic_rel_l1_l2_linf": res[ff.FF_FP64]["norms"],
+           "data": "analytic f (FishFry.hpp:22-44) + 64 seeded modes, |k| <= 32, a ~ N(0, 0.1), seed %d" % seed,
+           "steps": steps, "clocks": clk}
+    del res, p64, p32, diff
+    torch.cuda.empty_cache()
+    return out
+
+
+def extra_precision(args):
+    return precision_measure((1024, 1024, 1024), min(args.steps, 5), 3, args.seed)
+
+
+def run_precision(args):
+    """1024^3 FP32 solve of analytic f + 64 seeded modes; error against the
+    FP64 solve of the same input and against the analytic potential."""
+    n = tuple(args.grid) if args.grid != [512, 512, 512] else (1024, 1024, 1024)
+    r = precision_measure(n, args.steps, args.warmup, args.seed)
     line = {
-        "metric": "1024^3 FP32 solve points/s (precision form)", "value": N / (res[ff.FF_FP32]["ms"] * 1e-3),
+        "metric": "1024^3 FP32 solve points/s (precision form)", "value": r["fp32_points_per_s"],
         "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": res[ff.FF_FP32]["ms"], "higher_is_better": True, "dtype": "f32",
-        "data": "synthetic: analytic f (FishFry.hpp:22-44) + 64 seeded modes, |k| <= 32, a ~ N(0, 0.1)",
+        "ms_per_step": r["fp32_ms_per_solve"], "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic: " + r["data"],
         "config": {"workload": "%dx%dx%d FP32 (FP64 twiddles and 1/k^2)" % n, "modes_seed": args.seed},
-        "fp64_ms_per_solve": res[ff.FF_FP64]["ms"],
-        "fp32_vs_fp64_solve": {"rel_l2": rel_l2_dev(torch, p32, p64),
-                               "rel_linf": float(diff.abs().max() / p64.abs().max())},
-        "fp32_vs_analytic_rel_l1_l2_linf": res[ff.FF_FP32]["norms"],
-        "fp64_vs_analytic_rel_l1_l2_linf": res[ff.FF_FP64]["norms"],
     }
+    line.update({k: v for k, v in r.items() if k not in ("data",)})
     print(json.dumps(line), flush=True)
 
 
@@ -525,10 +585,11 @@ def batch_dims(seed=2024, count=256, choices=(32, 48, 64, 80, 96, 128)):
     return [tuple(int(x) for x in rng.choice(choices, 3)) for _ in range(count)]
 
 
-def run_batch(args):
+def batch_measure(steps, warmup, seed, tune=True):
     """256 grids with dims iid from {32, 48, 64, 80, 96, 128}: batched solves
     (five persistent launches, graph replay, tuned tiles) in FP64 and FP32
-    against a loop of single-grid FP64 solves of the same grids."""
+    against a loop of single-grid FP64 solves of the same grids; errors
+    against those plain FP64 solves, computed on the device."""
     import torch
 
     import fishfry_b200 as ff
@@ -536,21 +597,24 @@ def run_batch(args):
     pts = sum(a * b * c for a, b, c in dims)
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(device=dev)
-    K, W = args.steps, max(args.warmup, 3)
+    K, W = steps, max(warmup, 3)
     out = {}
     pristine = {}
+    clocks = ClockSampler(0)
     for prec in (ff.FF_FP64, ff.FF_FP32):
         dt = torch.float64 if prec == ff.FF_FP64 else torch.float32
         esz = 8 if prec == ff.FF_FP64 else 4
         b = ff.Batch(dims, precision=prec)
         d = [torch.empty(nb // esz, dtype=dt, device=dev) for nb in b.nbytes]
         p = [torch.empty(nb // esz, dtype=dt, device=dev) for nb in b.nbytes]
-        if not args.no_tune:
+        t_tune = time.perf_counter()
+        if tune:
             b.tune(d, p, stream=stream, reps=3)
+        t_tune = time.perf_counter() - t_tune
         f0 = []
         for g, n in enumerate(dims):
             x = torch.empty(n[0] * n[1] * n[2], dtype=dt, device=dev)
-            ff.init_field(n, x, modes_for(ff, n, args.seed + g), prec)
+            ff.init_field(n, x, modes_for(ff, n, seed + g), prec)
             f0.append(x)
         pristine[prec] = f0
 
@@ -561,6 +625,8 @@ def run_batch(args):
 
         tot = []
         for it in range(W + K):
+            if it == W and prec == ff.FF_FP32:
+                clocks.start()
             restore()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -569,13 +635,14 @@ def run_batch(args):
             e1.synchronize()
             if it >= W:
                 tot.append(e0.elapsed_time(e1))
+        b.check(stream)
         ms = sorted(tot)[len(tot) // 2]
         out[prec] = {"ms": ms, "solves_per_s": len(dims) / (ms * 1e-3), "points_per_s": pts / (ms * 1e-3),
-                     "phi": [x[:f.numel()].clone() for x, f in zip(p, f0)],
-                     "shapes": {k: b.shape(0, k) for k in range(5)}}
+                     "tune_s": t_tune, "phi": [x[:f.numel()].clone() for x, f in zip(p, f0)]}
         b.close()
         del d, p
         torch.cuda.empty_cache()
+    clk = clocks.stop()
     # loop of single-grid FP64 solves (the plain method, one plan per grid)
     plans = [ff.Plan(n) for n in dims]
     ds = [torch.empty(pl.nbytes // 8, dtype=torch.float64, device=dev) for pl in plans]
@@ -597,22 +664,41 @@ def run_batch(args):
     # accuracy: FP32 batch vs the plain FP64 solve; FP64 batch vs plain FP64
     err32 = max(rel_l2_dev(torch, a, y[:a.numel()]) for a, y in zip(out[ff.FF_FP32]["phi"], ps))
     err64 = max(rel_l2_dev(torch, a, y[:a.numel()]) for a, y in zip(out[ff.FF_FP64]["phi"], ps))
+    for pl in plans:
+        pl.close()
+    del ds, ps, pristine
     loop = {"ms": loop_ms, "solves_per_s": len(dims) / (loop_ms * 1e-3)}
-    line = {
-        "metric": "FP32 batched solves/s (256 grids, dims iid {32..128})",
-        "value": out[ff.FF_FP32]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": K, "warmup": W,
-        "ms_per_step": out[ff.FF_FP32]["ms"], "higher_is_better": True, "dtype": "f32",
-        "data": "synthetic: analytic f + 64 seeded modes per grid", "config": {
-            "workload": "256 grids, dims seed 2024, five persistent launches per solve (CUDA graph), %s tiles" % (
-                "default" if args.no_tune else "tuned"),
-            "points_per_batch": pts},
+    res = {
+        "grids": len(dims), "points_per_batch": pts, "steps": K, "tiles": "tuned" if tune else "default",
         "fp32_batch": {k: v for k, v in out[ff.FF_FP32].items() if k != "phi"},
         "fp64_batch": {k: v for k, v in out[ff.FF_FP64].items() if k != "phi"},
         "fp64_loop_of_plain_solves": loop,
         "fp32_batch_vs_fp64_loop": out[ff.FF_FP32]["solves_per_s"] / loop["solves_per_s"],
         "fp64_batch_vs_fp64_loop": out[ff.FF_FP64]["solves_per_s"] / loop["solves_per_s"],
         "max_rel_l2_vs_plain_fp64": {"fp32_batch": err32, "fp64_batch": err64},
+        "data": "analytic f + 64 seeded modes per grid (dims seed 2024, modes seed %d + grid index)" % seed,
+        "clocks": clk,
     }
+    del out
+    torch.cuda.empty_cache()
+    return res
+
+
+def extra_batch(args):
+    return batch_measure(min(args.steps, 10), 3, args.seed, tune=not args.no_tune)
+
+
+def run_batch(args):
+    r = batch_measure(args.steps, args.warmup, args.seed, tune=not args.no_tune)
+    line = {
+        "metric": "FP32 batched solves/s (256 grids, dims iid {32..128})",
+        "value": r["fp32_batch"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["fp32_batch"]["ms"], "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic: " + r["data"], "config": {
+            "workload": "256 grids, dims seed 2024, five persistent launches per solve (CUDA graph), %s tiles" %
+                        r["tiles"], "points_per_batch": r["points_per_batch"]},
+    }
+    line.update({k: v for k, v in r.items() if k not in ("data",)})
     print(json.dumps(line), flush=True)
 
 
@@ -642,88 +728,72 @@ def serve_dims(rng):
     return best[1]
 
 
-def run_serve(args):
-    """Poisson arrival stream of mixed-size FP32/FP64 requests through the
-    request loop; p50/p99 latency and solves/s per arrival rate."""
+def serve_stream(srv, reqs, gaps, src):
+    """Submits reqs = [(dims, precision)] with inter-arrival gaps (s) from a
+    producer thread, takes completions in completion order, releases them at
+    once, and returns the server's statistics of the stream."""
     import threading
+    srv.reset_stats()
+    ready = threading.Event()
 
-    import numpy as np
-    import torch
+    def producer():
+        t = time.perf_counter()
+        for q, (n, prec) in enumerate(reqs):
+            t += gaps[q]
+            while True:
+                now = time.perf_counter()
+                if now >= t:
+                    break
+                if t - now > 0.002:
+                    time.sleep(t - now - 0.001)
+            srv.submit(n, src[prec], prec)
+            if q == 0:
+                ready.set()
 
-    import fishfry_b200 as ff
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
+    th = threading.Thread(target=producer)
+    th.start()
+    ready.wait()
+    for _ in range(len(reqs)):
+        rid = srv.next()[0]
+        srv.release(rid)
+    th.join()
+    srv.check()
+    st = srv.stats()
+    return {"requests": len(reqs), "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+            "max_ms": st["max_ms"], "solves_per_s": st["solves_per_s"], "points_per_s": st["points_per_s"],
+            "completed": st["completed"], "peak_gb": st["peak_bytes"] / 1e9, "steps": st["steps"],
+            "launches": st["launches"], "max_active": st["max_active"]}
+
+
+def serve_sources(torch, ff, dev, seed):
+    """One device source field per precision: request inputs are read from it
+    (the solve's work does not depend on the values); the accuracy sample uses
+    proper fields."""
     gen = torch.Generator(device=dev)
-    gen.manual_seed(args.seed)
-    # request inputs are read from one device source field per precision (the
-    # solve's work does not depend on the values); the accuracy sample below
-    # uses proper fields
-    src = {ff.FF_FP64: torch.randn(512 ** 3, dtype=torch.float64, device=dev, generator=gen),
-           ff.FF_FP32: torch.randn(512 ** 3, dtype=torch.float32, device=dev, generator=gen)}
-    results = []
-    for rate in args.rates:
-        t_rate = time.perf_counter()
-        rng = np.random.default_rng(args.seed + int(rate))
-        reqs = [(serve_dims(rng), int(rng.integers(2))) for _ in range(args.requests)]
-        print("serve rate %g: %d requests drawn in %.1f s" % (rate, len(reqs), time.perf_counter() - t_rate),
-              file=sys.stderr, flush=True)
-        gaps = rng.exponential(1.0 / rate, args.requests)
-        srv = ff.Server(int(args.budget_gb * 1e9), max_active=4096)
-        # warm-up: every axis length's tables resident in both precisions
-        warm = []
-        for L in SMOOTH:
-            for prec in (ff.FF_FP64, ff.FF_FP32):
-                warm.append(srv.submit((L, 32, 32), src[prec], prec))
-        for rid in warm:
-            srv.wait(rid)
-            srv.release(rid)
-        srv.reset_stats()
-        ids = [None] * len(reqs)
-        ready = threading.Event()
+    gen.manual_seed(seed)
+    return {ff.FF_FP64: torch.randn(512 ** 3, dtype=torch.float64, device=dev, generator=gen),
+            ff.FF_FP32: torch.randn(512 ** 3, dtype=torch.float32, device=dev, generator=gen)}
 
-        def producer():
-            t0 = time.perf_counter()
-            t = t0
-            for q, (n, prec) in enumerate(reqs):
-                t += gaps[q]
-                while True:
-                    now = time.perf_counter()
-                    if now >= t:
-                        break
-                    if t - now > 0.002:
-                        time.sleep(t - now - 0.001)
-                ids[q] = srv.submit(n, src[prec], prec)
-                if q == 0:
-                    ready.set()
 
-        th = threading.Thread(target=producer)
-        th.start()
-        ready.wait()
-        # completions are taken in completion order and released at once (a
-        # finished request holds its buffers until released)
-        for _ in range(len(reqs)):
-            rid = srv.next()[0]
-            srv.release(rid)
-        th.join()
-        st = srv.stats()
-        srv.close()
-        print("serve rate %g: %d requests in %.1f s, p50 %.3f ms, p99 %.3f ms, %.0f solves/s" % (
-            rate, st["completed"], time.perf_counter() - t_rate, st["p50_ms"], st["p99_ms"], st["solves_per_s"]),
-            file=sys.stderr, flush=True)
-        results.append({"rate": rate, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-                        "max_ms": st["max_ms"], "solves_per_s": st["solves_per_s"],
-                        "points_per_s": st["points_per_s"], "completed": st["completed"],
-                        "peak_gb": st["peak_bytes"] / 1e9, "steps": st["steps"], "launches": st["launches"],
-                        "max_active": st["max_active"]})
-    # the plain method on the same mix: single-grid solves one after another
-    # (plans made beforehand, each request's field copied in first, as the
-    # server copies it), FP64 and FP32, on a sample of the request stream
-    rng = np.random.default_rng(args.seed + 7)
-    sample = [serve_dims(rng) for _ in range(min(400, args.requests))]
+def serve_warm(srv, ff, src):
+    """Every axis length's tables resident in both precisions."""
+    warm = []
+    for L in SMOOTH:
+        for prec in (ff.FF_FP64, ff.FF_FP32):
+            warm.append(srv.submit((L, 32, 32), src[prec], prec))
+    for rid in warm:
+        srv.wait(rid)
+        srv.release(rid)
+
+
+def serve_plain_loops(torch, ff, dev, dims, src):
+    """The plain method on the same requests: single-grid solves one after
+    another (plans made beforehand; each request's field copied in first, as
+    the server copies it), FP64 and FP32; solves/s of the second pass."""
     plain = {}
     for prec in (ff.FF_FP64, ff.FF_FP32):
         dt = torch.float64 if prec == ff.FF_FP64 else torch.float32
-        plans = {n: ff.Plan(n, precision=prec) for n in set(sample)}
+        plans = {n: ff.Plan(n, precision=prec) for n in set(dims)}
         cap = max(pl.nbytes for pl in plans.values())
         esz = 8 if prec == ff.FF_FP64 else 4
         d = torch.empty(cap // esz, dtype=dt, device=dev)
@@ -732,7 +802,7 @@ def run_serve(args):
         for rep in range(2):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(st)
-            for n in sample:
+            for n in dims:
                 N = n[0] * n[1] * n[2]
                 with torch.cuda.stream(st):
                     d[:N].copy_(src[prec][:N])
@@ -740,23 +810,32 @@ def run_serve(args):
             e1.record(st)
             e1.synchronize()
         ms = e0.elapsed_time(e1)
-        plain["fp64" if prec == ff.FF_FP64 else "fp32"] = {"solves_per_s": len(sample) / (ms * 1e-3),
-                                                           "requests": len(sample)}
+        plain["fp64" if prec == ff.FF_FP64 else "fp32"] = {"solves_per_s": len(dims) / (ms * 1e-3),
+                                                           "requests": len(dims)}
         for pl in plans.values():
             pl.close()
         del d, p
         torch.cuda.empty_cache()
-    # accuracy sample: FP32 requests against the plain FP64 solve of the same f
-    srv = ff.Server(int(min(args.budget_gb, 40) * 1e9), max_active=64)
-    rng = np.random.default_rng(args.seed)
+    return plain
+
+
+def serve_accuracy(torch, ff, dev, seed, budget_gb, count=8, max_points=256 ** 3):
+    """FP32 requests through the server against the plain FP64 solve of the
+    same f (analytic + 64 seeded modes); the worst relative L2."""
+    import numpy as np
+    srv = ff.Server(int(min(budget_gb, 40) * 1e9), max_active=64)
+    rng = np.random.default_rng(seed)
     worst = 0.0
-    for q in range(8):
+    checked = 0
+    for q in range(4 * count):
+        if checked == count:
+            break
         n = serve_dims(rng)
-        if n[0] * n[1] * n[2] > 256 ** 3:
-            continue
         N = n[0] * n[1] * n[2]
+        if N > max_points:
+            continue
         f64 = torch.empty(N, dtype=torch.float64, device=dev)
-        ff.init_field(n, f64, modes_for(ff, n, args.seed + q), ff.FF_FP64)
+        ff.init_field(n, f64, modes_for(ff, n, seed + q), ff.FF_FP64)
         f32 = f64.float()
         rid = srv.submit(n, f32, ff.FF_FP32)
         srv.wait(rid)
@@ -768,7 +847,95 @@ def run_serve(args):
         d[:N].copy_(f32.double())
         plan.solve(d, p)
         worst = max(worst, rel_l2_dev(torch, o32, p[:N]))
+        plan.close()
+        checked += 1
     srv.close()
+    return worst, checked
+
+
+def serve_measure(seed, budget_gb, requests, rate_low=1000.0, rate_sat=5000.0, plain_sample=400):
+    """Short request streams through one server: the 1:1 FP32:FP64 mix at
+    rate_low (latency) and at rate_sat (saturation, solves/s), the FP32 lane
+    alone at rate_sat on the same dims, and the plain FP64 / FP32 loops over
+    those dims."""
+    import numpy as np
+    import torch
+
+    import fishfry_b200 as ff
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    src = serve_sources(torch, ff, dev, seed)
+    srv = ff.Server(int(budget_gb * 1e9), max_active=4096)
+    serve_warm(srv, ff, src)
+    rng = np.random.default_rng(seed + 1000)
+    low = [(serve_dims(rng), int(rng.integers(2))) for _ in range(requests)]
+    gaps_low = rng.exponential(1.0 / rate_low, requests)
+    sat = [(serve_dims(rng), int(rng.integers(2))) for _ in range(requests)]
+    gaps_sat = rng.exponential(1.0 / rate_sat, requests)
+    clocks = ClockSampler(0)
+    clocks.start()
+    r_low = serve_stream(srv, low, gaps_low, src)
+    r_sat = serve_stream(srv, sat, gaps_sat, src)
+    r_32 = serve_stream(srv, [(n, ff.FF_FP32) for n, _ in sat], gaps_sat, src)
+    clk = clocks.stop()
+    srv.close()
+    dims = [n for n, _ in sat[:plain_sample]]
+    plain = serve_plain_loops(torch, ff, dev, dims, src)
+    del src
+    torch.cuda.empty_cache()
+    worst, checked = serve_accuracy(torch, ff, dev, seed, budget_gb)
+    r_low["rate"] = rate_low
+    r_sat["rate"] = rate_sat
+    r_32["rate"] = rate_sat
+    return {
+        "mix_1to1_at_%g_per_s" % rate_low: r_low,
+        "mix_1to1_at_%g_per_s" % rate_sat: r_sat,
+        "fp32_only_at_%g_per_s" % rate_sat: r_32,
+        "plain_loop_on_the_saturation_dims": plain,
+        "p50_ms_at_%g_per_s" % rate_low: r_low["p50_ms"], "p99_ms_at_%g_per_s" % rate_low: r_low["p99_ms"],
+        "served_mix_vs_plain_fp64": r_sat["solves_per_s"] / plain["fp64"]["solves_per_s"],
+        "served_fp32_vs_plain_fp64": r_32["solves_per_s"] / plain["fp64"]["solves_per_s"],
+        "fp32_vs_plain_fp64_rel_l2_max": worst, "accuracy_requests": checked,
+        "budget_gb": budget_gb,
+        "data": "request dims log-uniform in points (5-smooth, 32..512 per axis), seed %d" % seed,
+        "clocks": clk,
+    }
+
+
+def extra_serve(args):
+    return serve_measure(args.seed, args.budget_gb, requests=min(args.requests, 1500))
+
+
+def run_serve(args):
+    """Poisson arrival stream of mixed-size FP32/FP64 requests through the
+    request loop; p50/p99 latency and solves/s per arrival rate."""
+    import numpy as np
+    import torch
+
+    import fishfry_b200 as ff
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    src = serve_sources(torch, ff, dev, args.seed)
+    results = []
+    for rate in args.rates:
+        t_rate = time.perf_counter()
+        rng = np.random.default_rng(args.seed + int(rate))
+        reqs = [(serve_dims(rng), int(rng.integers(2))) for _ in range(args.requests)]
+        gaps = rng.exponential(1.0 / rate, args.requests)
+        srv = ff.Server(int(args.budget_gb * 1e9), max_active=4096)
+        serve_warm(srv, ff, src)
+        r = serve_stream(srv, reqs, gaps, src)
+        srv.close()
+        r["rate"] = rate
+        print("serve rate %g: %d requests in %.1f s, p50 %.3f ms, p99 %.3f ms, %.0f solves/s" % (
+            rate, r["completed"], time.perf_counter() - t_rate, r["p50_ms"], r["p99_ms"], r["solves_per_s"]),
+            file=sys.stderr, flush=True)
+        results.append(r)
+    rng = np.random.default_rng(args.seed + 7)
+    plain = serve_plain_loops(torch, ff, dev, [serve_dims(rng) for _ in range(min(400, args.requests))], src)
+    del src
+    torch.cuda.empty_cache()
+    worst, checked = serve_accuracy(torch, ff, dev, args.seed, args.budget_gb)
     line = {
         "metric": "served solves/s and p99 latency (Poisson arrivals, dims 32..512, FP32:FP64 1:1)",
         "value": max(r["solves_per_s"] for r in results), "unit": "solves/s", "n_gpus": 1,
@@ -779,7 +946,7 @@ def run_serve(args):
         "rates": results,
         "plain_loop_on_the_same_mix": plain,
         "served_at_saturation_vs_plain_fp64": max(r["solves_per_s"] for r in results) / plain["fp64"]["solves_per_s"],
-        "fp32_vs_plain_fp64_rel_l2_max": worst,
+        "fp32_vs_plain_fp64_rel_l2_max": worst, "accuracy_requests": checked,
     }
     print(json.dumps(line), flush=True)
 

@@ -26,7 +26,7 @@ FF_MAX_AXIS = 1800
 # Every symbol include/fishfry.h declares.
 EXPORTS = [
     "ff_phase_name", "ff_plan_phases", "ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check",
-    "ff_plan_destroy", "ff_solve_passes",
+    "ff_plan_destroy", "ff_solve_passes", "ff_plan_set_wait_limit",
     "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_status_string",
     "ff_last_error", "ff_version",
     "ff_batch_create", "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
@@ -88,6 +88,7 @@ def _declare(L):
     L.ff_plan_check.argtypes = [vp, vp]
     L.ff_solve_passes.argtypes = [vp, ctypes.c_size_t, vp, vp, vp, ctypes.c_int]
     L.ff_plan_destroy.argtypes = [vp]
+    L.ff_plan_set_wait_limit.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     L.ff_init_field.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, vp]
     L.ff_error_sums.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, d3, vp]
     L.ff_error_sums_noalloc.argtypes = [i3, d3, d3, ctypes.c_int, vp, ctypes.c_int, vp, d3, vp]
@@ -121,7 +122,7 @@ def _declare(L):
                  "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy"):
         getattr(L, name).restype = ctypes.c_int
     for name in ("ff_plan_create", "ff_plan_bytes", "ff_plan_info", "ff_solve", "ff_plan_check", "ff_plan_destroy",
-                 "ff_solve_passes",
+                 "ff_solve_passes", "ff_plan_set_wait_limit",
                  "ff_init_field", "ff_error_sums", "ff_error_sums_noalloc", "ff_modes_generate", "ff_batch_create",
                  "ff_batch_bytes", "ff_batch_solve", "ff_batch_tune", "ff_batch_shape", "ff_batch_check",
                  "ff_batch_destroy", "ff_batch_radices"):

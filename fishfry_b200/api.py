@@ -89,6 +89,12 @@ class Plan:
         """Raises FFError(FF_ERR_TIMEOUT) if a kernel's bounded wait gave up."""
         check(lib().ff_plan_check(self._h, _stream(stream)), "ff_plan_check")
 
+    def set_wait_limit(self, iterations=0, target_extra=0):
+        """Test hook (ff_plan_set_wait_limit): iteration limit of the bounded
+        device waits (0: built-in) and an extra producer count added to the
+        fused passes' dependency waits (1 makes them run out)."""
+        check(lib().ff_plan_set_wait_limit(self._h, int(iterations), int(target_extra)), "ff_plan_set_wait_limit")
+
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             check(lib().ff_plan_destroy(self._h), "ff_plan_destroy")
@@ -271,15 +277,20 @@ class ParisPencil:
         return self._plan.nbytes
 
     def solve(self, bytes, density, potential, stamps):
-        """Overwrites `stamps` with [("Total", t0), (phase, t), ...]; blocks until done."""
+        """Overwrites `stamps` with [("Total", t0), (phase, t), ...]; blocks
+        until done.  As in the reference (ParisPencil.cpp:98, :424) the last
+        stamp minus the first is the host wall time of the whole solve; the
+        phases in between are placed by their CUDA-event durations."""
         stamps.clear()
         t0 = time.monotonic()
         stamps.append(("Total", t0))
         ms, _ = self._plan.solve(density, potential, nbytes=bytes, timed=True)
+        t1 = time.monotonic()
         t = t0
-        for name, dt in zip(phase_names(self._plan), ms):
+        names = phase_names(self._plan)
+        for q, (name, dt) in enumerate(zip(names, ms)):
             t += 1e-3 * dt
-            stamps.append((name, t))
+            stamps.append((name, max(t, t1) if q + 1 == len(ms) else t))
 
 
 def init_field(n, f, modes=None, precision=FF_FP64, stream=None):

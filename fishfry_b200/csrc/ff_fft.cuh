@@ -599,10 +599,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *m, uint32_t parity) {
   return ok != 0;
 }
 
-// Waits for phase `parity` of m with an iteration limit (about a second with
-// the back-off); returns false if the limit ran out.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *m, uint32_t parity) {
-  for (int i = 0; i < (1 << 24); i++) {
+// Built-in iteration limit of the bounded waits (about a second with the
+// back-off of mbar_wait_bounded).
+constexpr int kWaitIters = 1 << 24;
+
+// Waits for phase `parity` of m with an iteration limit (limit <= 0: the
+// built-in kWaitIters); returns false if the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *m, uint32_t parity, int limit = kWaitIters) {
+  if (limit <= 0) limit = kWaitIters;
+  for (int i = 0; i < limit; i++) {
     if (mbar_try_wait(m, parity)) return true;
     if (i >= 32) __nanosleep(64);
   }

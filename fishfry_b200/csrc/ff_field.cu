@@ -187,20 +187,31 @@ static unsigned grid_for(long N, int threads) {
 // file-scope device array instead of a per-call buffer: every GPU that loads
 // this library holds it (about 384 KB) until the process exits.
 //
-// Each block reduces one contiguous chunk of kNoAllocChunk points in a fixed
-// order, so the number of partials, and the array's size, bound the grid:
-// at most kNoAllocMaxChunks * kNoAllocChunk = 2^30 points (1024^3).
-constexpr long kNoAllocChunk = 65536;
+// Each block reduces one contiguous chunk of points in a fixed order.  The
+// chunk length is a function of N alone (about N / kNoAllocBlocks, a multiple
+// of kSumThreads), so small grids still spread over every SM and the
+// summation order is the same on every call for a given grid.  The grid is
+// limited to kNoAllocMaxPoints = 2^30 points (1024^3); the array holds the
+// partials of at most kNoAllocMaxChunks blocks plus the final triple.
+constexpr int kNoAllocBlocks = 8 * 148;
 constexpr int kNoAllocMaxChunks = 16384;
+constexpr long kNoAllocMaxPoints = 1L << 30;
 static __device__ __align__(256) double g_noalloc_partials[3 * kNoAllocMaxChunks + 3];
+
+// Chunk length for a grid of N points: ceil(N / kNoAllocBlocks) rounded up to
+// a multiple of kSumThreads; chunks = ceil(N / chunk) <= kNoAllocBlocks.
+static long noalloc_chunk(long N) {
+  long c = (N + kNoAllocBlocks - 1) / kNoAllocBlocks;
+  return (c + kSumThreads - 1) / kSumThreads * kSumThreads;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(kSumThreads) k_diff_chunks(const FieldArgs a, const T *__restrict__ phi,
-                                                             double *__restrict__ partial) {
+                                                             long chunk, double *__restrict__ partial) {
   __shared__ double s1[kSumThreads], s2[kSumThreads], sm[kSumThreads];
   const long N = (long)a.ni * a.nj * a.nk;
-  const long q0 = (long)blockIdx.x * kNoAllocChunk;
-  const long q1 = q0 + kNoAllocChunk < N ? q0 + kNoAllocChunk : N;
+  const long q0 = (long)blockIdx.x * chunk;
+  const long q1 = q0 + chunk < N ? q0 + chunk : N;
   double t1 = 0, t2 = 0, tm = 0;
   for (long q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
     const int k = (int)(q % a.nk);
@@ -237,7 +248,9 @@ __global__ void __launch_bounds__(kSumThreads) k_diff_chunks(const FieldArgs a, 
 
 // Device address of g_noalloc_partials on the current device.  The name is a
 // host-side stand-in, not a device address, so it is looked up once per
-// device (with that device current) and remembered.
+// device (with that device current) and remembered.  A cudaDeviceReset in the
+// process makes the remembered address stale (the module is reloaded, perhaps
+// elsewhere): the entry point is not for use after a reset.
 static int noalloc_partials(double **out) {
   static std::mutex mu;
   static void *addr[256] = {};
@@ -318,20 +331,25 @@ int ff_error_sums_noalloc(const int n[3], const double xlo[3], const double dx[3
   if (precision != FF_FP64 && precision != FF_FP32)
     return set_error(FF_ERR_INVALID, "ff_error_sums_noalloc: bad precision %d", precision);
   const long N = (long)n[0] * n[1] * n[2];
-  const long chunks = (N + kNoAllocChunk - 1) / kNoAllocChunk;
-  if (chunks > kNoAllocMaxChunks)
+  if (N > kNoAllocMaxPoints)
     return set_error(FF_ERR_UNSUPPORTED,
-                     "ff_error_sums_noalloc: %ld points exceed the fixed partial-sum array (at most %ld points)", N,
-                     (long)kNoAllocMaxChunks * kNoAllocChunk);
+                     "ff_error_sums_noalloc: %ld points exceed the fixed partial-sum array's limit of %ld points", N,
+                     kNoAllocMaxPoints);
+  const long chunk = noalloc_chunk(N);
+  const long chunks = (N + chunk - 1) / chunk;
+  if (chunks > kNoAllocMaxChunks)   // cannot happen for N <= kNoAllocMaxPoints; kept as the array's guard
+    return set_error(FF_ERR_UNSUPPORTED, "ff_error_sums_noalloc: %ld chunks exceed the fixed array", chunks);
   double *partial = nullptr;
   rc = noalloc_partials(&partial);
   if (rc != FF_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // every slot read below is written by this call first: nothing to clear
   if (precision == FF_FP64)
-    k_diff_chunks<double><<<(unsigned)chunks, kSumThreads, 0, st>>>(a, static_cast<const double *>(phi), partial);
+    k_diff_chunks<double><<<(unsigned)chunks, kSumThreads, 0, st>>>(a, static_cast<const double *>(phi), chunk,
+                                                                    partial);
   else
-    k_diff_chunks<float><<<(unsigned)chunks, kSumThreads, 0, st>>>(a, static_cast<const float *>(phi), partial);
+    k_diff_chunks<float><<<(unsigned)chunks, kSumThreads, 0, st>>>(a, static_cast<const float *>(phi), chunk,
+                                                                   partial);
   double *total = partial + 3 * kNoAllocMaxChunks;
   k_diff_final<<<1, kSumThreads, 0, st>>>(partial, (int)chunks, total);
   cudaError_t e = cudaGetLastError();

@@ -87,7 +87,9 @@ struct Arena {
   }
 };
 
-enum ReqState { kPending, kLoading, kRunning, kDone };
+// kFetching: a finished request whose result ff_server_fetch is copying out;
+// its buffers stay reserved until that copy has completed.
+enum ReqState { kPending, kLoading, kRunning, kDone, kFetching };
 
 struct Request {
   uint64_t id = 0;
@@ -480,6 +482,26 @@ void scheduler(ff_server *s) {
 }  // namespace
 }  // namespace ff
 
+// Frees a pending or finished request's buffers and slot and forgets it; the
+// caller holds s->mu.
+template <typename It> static void release_locked(ff_server *s, It it) {
+  Request &q = it->second;
+  if (q.state == kPending) {
+    s->pending.erase(std::find(s->pending.begin(), s->pending.end(), q.id));
+  } else {
+    s->arena.release(q.off_d, q.bytes);
+    s->arena.release(q.off_p, q.bytes);
+    s->lane[q.precision == FF_FP64 ? 0 : 1].free_slots.push_back(q.slot);
+    s->admit_dirty = true;
+  }
+  if (q.in_ev) cudaEventDestroy(q.in_ev);
+  s->reqs.erase(it);
+}
+
+// Waits longer than this (about 31 years) are waits without limit; it keeps
+// the deadline arithmetic in range for INFINITY and other huge values.
+constexpr double kMaxTimeoutMs = 1e12;
+
 extern "C" {
 
 int ff_server_create(const ff_server_config *cfg, ff_server **out) {
@@ -555,7 +577,8 @@ int ff_server_submit(ff_server *s, const int n[3], int precision, const void *f,
 int ff_server_wait(ff_server *s, uint64_t id, double timeout_ms, ff_request_info *info) {
   if (!s) return set_error(FF_ERR_INVALID, "ff_server_wait: null server");
   std::unique_lock<std::mutex> lk(s->mu);
-  const auto deadline = Clock::now() + std::chrono::microseconds((long long)(timeout_ms * 1000.0));
+  const bool bounded = timeout_ms >= 0 && timeout_ms < kMaxTimeoutMs;
+  const auto deadline = Clock::now() + std::chrono::microseconds(bounded ? (long long)(timeout_ms * 1000.0) : 0);
   for (;;) {
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return set_error(FF_ERR_INVALID, "ff_server_wait: unknown request %llu",
@@ -570,9 +593,9 @@ int ff_server_wait(ff_server *s, uint64_t id, double timeout_ms, ff_request_info
       return FF_OK;
     }
     if (s->fatal != FF_OK) return set_error(s->fatal, "ff_server_wait: server stopped: %s", s->fatal_msg);
-    if (timeout_ms >= 0 && Clock::now() >= deadline)
+    if (bounded && Clock::now() >= deadline)
       return set_error(FF_ERR_TIMEOUT, "ff_server_wait: request %llu not done", (unsigned long long)id);
-    if (timeout_ms >= 0) s->cv_done.wait_until(lk, deadline);
+    if (bounded) s->cv_done.wait_until(lk, deadline);
     else s->cv_done.wait(lk);
   }
 }
@@ -580,7 +603,8 @@ int ff_server_wait(ff_server *s, uint64_t id, double timeout_ms, ff_request_info
 int ff_server_next(ff_server *s, double timeout_ms, uint64_t *id, ff_request_info *info) {
   if (!s || !id) return set_error(FF_ERR_INVALID, "ff_server_next: null argument");
   std::unique_lock<std::mutex> lk(s->mu);
-  const auto deadline = Clock::now() + std::chrono::microseconds((long long)(timeout_ms * 1000.0));
+  const bool bounded = timeout_ms >= 0 && timeout_ms < kMaxTimeoutMs;
+  const auto deadline = Clock::now() + std::chrono::microseconds(bounded ? (long long)(timeout_ms * 1000.0) : 0);
   for (;;) {
     while (!s->finished.empty()) {
       const uint64_t q = s->finished.front();
@@ -597,9 +621,9 @@ int ff_server_next(ff_server *s, double timeout_ms, uint64_t *id, ff_request_inf
       return FF_OK;
     }
     if (s->fatal != FF_OK) return set_error(s->fatal, "ff_server_next: server stopped: %s", s->fatal_msg);
-    if (timeout_ms >= 0 && Clock::now() >= deadline)
+    if (bounded && Clock::now() >= deadline)
       return set_error(FF_ERR_TIMEOUT, "ff_server_next: no request finished");
-    if (timeout_ms >= 0) s->cv_done.wait_until(lk, deadline);
+    if (bounded) s->cv_done.wait_until(lk, deadline);
     else s->cv_done.wait(lk);
   }
 }
@@ -609,20 +633,37 @@ int ff_server_fetch(ff_server *s, uint64_t id, void *phi, int phi_on_host) {
   void *src = nullptr;
   size_t bytes = 0;
   {
+    // claim the request: a concurrent fetch or release of the same id is
+    // refused until the copy below has finished, so its buffers cannot be
+    // handed to another request while they are being read
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return set_error(FF_ERR_INVALID, "ff_server_fetch: unknown request");
+    if (it->second.state == kFetching)
+      return set_error(FF_ERR_INVALID, "ff_server_fetch: request %llu is being fetched by another call",
+                       (unsigned long long)id);
     if (it->second.state != kDone) return set_error(FF_ERR_INVALID, "ff_server_fetch: request not done");
-    const Request &q = it->second;
+    Request &q = it->second;
+    q.state = kFetching;
     src = q.g.potential;
     bytes = (size_t)q.n[0] * q.n[1] * q.n[2] * (q.precision == FF_FP64 ? 8 : 4);
   }
+  cudaError_t e = cudaSuccess;
   if (phi) {
-    FF_CUDA(cudaMemcpyAsync(phi, src, bytes, phi_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
-                            s->fetch));
-    FF_CUDA(cudaStreamSynchronize(s->fetch));
+    e = cudaMemcpyAsync(phi, src, bytes, phi_on_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s->fetch);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->fetch);
   }
-  return ff_server_release(s, id);
+  {
+    // the claim ends: the request is released in the same critical section,
+    // so no other call can see it between the copy and the release
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(id);
+    if (it != s->reqs.end()) release_locked(s, it);
+  }
+  s->cv_work.notify_one();
+  if (e != cudaSuccess)
+    return set_error(FF_ERR_CUDA, "ff_server_fetch: %s (%s)", cudaGetErrorName(e), cudaGetErrorString(e));
+  return FF_OK;
 }
 
 int ff_server_release(ff_server *s, uint64_t id) {
@@ -631,18 +672,11 @@ int ff_server_release(ff_server *s, uint64_t id) {
   auto it = s->reqs.find(id);
   if (it == s->reqs.end()) return set_error(FF_ERR_INVALID, "ff_server_release: unknown request");
   Request &q = it->second;
+  if (q.state == kFetching)
+    return set_error(FF_ERR_INVALID, "ff_server_release: request %llu is being fetched", (unsigned long long)id);
   if (q.state != kDone && q.state != kPending)
     return set_error(FF_ERR_INVALID, "ff_server_release: request %llu is on the device", (unsigned long long)id);
-  if (q.state == kPending) {
-    s->pending.erase(std::find(s->pending.begin(), s->pending.end(), id));
-  } else {
-    s->arena.release(q.off_d, q.bytes);
-    s->arena.release(q.off_p, q.bytes);
-    s->lane[q.precision == FF_FP64 ? 0 : 1].free_slots.push_back(q.slot);
-    s->admit_dirty = true;
-  }
-  if (q.in_ev) cudaEventDestroy(q.in_ev);
-  s->reqs.erase(it);
+  release_locked(s, it);
   s->cv_work.notify_one();
   return FF_OK;
 }

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, 
     if (a.l2_ahead > 0 && fl < nlines)
       l2_prefetch(f + fl * a.nk, (uint32_t)(min((long)(2 * W), nlines - fl) * a.nk * sizeof(T)));
   }
-  const ZTileIO io{&mbar, 0, a.status};
+  const ZTileIO io{&mbar, 0, a.status, a.wait_iters};
   z_fwd_tile<T, N, BULK, true>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                                reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zinv(const typename Cplx<T>::t
       l2_prefetch(spec + fl * a.nhp,
                   (uint32_t)(min((long)(2 * W), nlines - fl) * a.nhp * sizeof(typename Cplx<T>::type)));
   }
-  const ZTileIO io{&mbar, 0, a.status};
+  const ZTileIO io{&mbar, 0, a.status, a.wait_iters};
   z_inv_tile<T, N, BULK>(spec, out, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                          reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(kZThreads, 3)
     mbar_init_fence();
   }
   __syncthreads();
-  if (!tma_tile<C, W, XPASS>(&tmap, sm, &mbar, 0, n, box_rows, o, kt, a.status)) return;
+  if (!tma_tile<C, W, XPASS>(&tmap, sm, &mbar, 0, n, box_rows, o, kt, a.status, a.wait_iters)) return;
   if (XPASS) {
     x_tile<T, W, N>(&tmap, a, o, kt, box_rows, sm);
   } else {
@@ -198,7 +198,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kZThreads, 3)
     }
   }
   __syncthreads();
-  bool ok = mbar_wait_bounded(&mbar, 0);
+  bool ok = mbar_wait_bounded(&mbar, 0, a.wait_iters);
   ok = !__syncthreads_or(!ok);
   if (!ok && threadIdx.x == 0) {
     // report; the block still takes part in every cluster barrier below (its
@@ -284,6 +284,8 @@ struct FuseArgs {
   int lag;         // planes between a producer tile and its plane's consumers (<= planes)
   int zW, zP;      // z tile shape
   int box_rows;    // TMA box rows of y tiles
+  int wait_iters;  // iteration limit of a dependency wait (0: built-in)
+  int target_extra;  // added to every dependency wait's target (0; a test sets 1 to make the waits run out)
 };
 
 __device__ __forceinline__ void fuse_decode(const FuseArgs &f, int t, bool &cons, int &plane, int &tile) {
@@ -310,9 +312,14 @@ __device__ __forceinline__ void fuse_decode(const FuseArgs &f, int t, bool &cons
   tile = t - (t / B) * B;
 }
 
-// Bounded wait for *p >= target (acquire at GPU scope).
-__device__ __forceinline__ bool wait_count(const int *p, int target) {
-  for (int i = 0; i < (1 << 22); i++) {
+// Built-in iteration limit of a dependency wait (about a second).
+constexpr int kDepWaitIters = 1 << 22;
+
+// Bounded wait for *p >= target (acquire at GPU scope); limit <= 0: the
+// built-in kDepWaitIters.
+__device__ __forceinline__ bool wait_count(const int *p, int target, int limit) {
+  if (limit <= 0) limit = kDepWaitIters;
+  for (int i = 0; i < limit; i++) {
     int v;
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     if (v >= target) return true;
@@ -328,11 +335,12 @@ __device__ __forceinline__ void publish(int *done, int plane) {
   if (threadIdx.x == 0) atomicAdd(done + plane, 1);
 }
 
-// Waits for all producer tiles of `plane`; false on every thread on timeout.
+// Waits for all producer tiles of `plane`; false on every thread on timeout,
+// and the caller then leaves without touching the plane.
 __device__ __forceinline__ bool await_plane(const FuseArgs &fa, int plane, int *status) {
   bool ok = true;
   if (threadIdx.x == 0) {
-    ok = wait_count(fa.done + plane, fa.prod_pp);
+    ok = wait_count(fa.done + plane, fa.prod_pp + fa.target_extra, fa.wait_iters);
     if (!ok) atomicExch(status, kDevDepTimeout);
   }
   return !__syncthreads_or(!ok);
@@ -363,7 +371,7 @@ __global__ void __launch_bounds__(kZThreads, 3)
     if (!cons) {
       const long first = (long)plane * a.nj;
       z_fwd_tile<T, NZ, false>(f, spec, a, fa.zW, fa.zP, first + (long)tile * 2 * fa.zW, first + a.nj, sm,
-                               ZTileIO{nullptr, 0, a.status});
+                               ZTileIO{nullptr, 0, a.status, 0});
       publish(fa.done, plane);
     } else {
       if (!await_plane(fa, plane, a.status)) break;
@@ -408,7 +416,9 @@ __global__ void __launch_bounds__(kZThreads, 3)
       // launch, so TMA may read it)
       fence_proxy_async_smem();
       __syncthreads();
-      if (!tma_tile<C, W, false>(&tmap, sm, &mbar, loads & 1, ny, fa.box_rows, plane, tile, a.status)) break;
+      if (!tma_tile<C, W, false>(&tmap, sm, &mbar, loads & 1, ny, fa.box_rows, plane, tile, a.status,
+                                 a.wait_iters))
+        break;
       loads++;
       PointTile<W, C> tl{sm};
       y_tile<T, W, true, NY>(tl, specD, a, plane, tile, sm);
@@ -417,7 +427,7 @@ __global__ void __launch_bounds__(kZThreads, 3)
       if (!await_plane(fa, plane, a.status)) break;
       const long first = (long)plane * a.nj;
       z_inv_tile<T, NZ, false>(specD, out, a, fa.zW, fa.zP, first + (long)tile * 2 * fa.zW, first + a.nj, sm,
-                               ZTileIO{nullptr, 0, a.status});
+                               ZTileIO{nullptr, 0, a.status, 0});
     }
   }
 }
@@ -487,6 +497,8 @@ struct ff_plan {
   size_t zsmem;
   unsigned ztiles;
   int l2_ahead;        // forward z pass: L2 prefetch distance in blocks (0: off)
+  int wait_iters;      // bounded device waits: iteration limit of the first wait (0: built-in)
+  int dep_extra;       // fused passes: added to every dependency wait's target (test hook, 0)
   StridedCfg ycfg, xcfg;
   FusedCfg fwd, inv;
   // axes with a prime factor above 7: padded convolution length M (0 for a
@@ -795,6 +807,7 @@ template <typename T> static PassArgs<T> pass_args(const ff_plan *p) {
   for (int d = 0; d < 3; d++) a.dd[d] = p->dd[d];
   a.status = p->status;
   a.l2_ahead = p->l2_ahead;
+  a.wait_iters = p->wait_iters;
   return a;
 }
 
@@ -822,7 +835,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     const int ni = p->n[0];
     FF_CUDA(cudaMemsetAsync(p->counters, 0, (2 + 2 * (size_t)ni) * sizeof(int), st));
     FuseArgs ff{p->counters, p->counters + 2, ni, p->fwd.prod_pp, p->fwd.cons_pp, p->fwd.lag, p->zW, p->zP,
-                p->ycfg.box_rows};
+                p->ycfg.box_rows, p->wait_iters, p->dep_extra};
     fwd_kernel<T>(p->fwd.NZ, p->fwd.NY)<<<p->fwd.grid, kZThreads, p->fwd.smem, st>>>(D, Ps, a, ff);
     FF_CUDA(cudaGetLastError());
     if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
@@ -830,7 +843,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     FF_CUDA(cudaGetLastError());
     if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
     FuseArgs fi{p->counters + 1, p->counters + 2 + ni, ni, p->inv.prod_pp, p->inv.cons_pp, p->inv.lag, p->zW, p->zP,
-                p->ycfg.box_rows};
+                p->ycfg.box_rows, p->wait_iters, p->dep_extra};
     inv_kernel<T>(p->inv.NZ, p->inv.NY)<<<p->inv.grid, kZThreads, p->inv.smem, st>>>(ymapP, Ds, P, a, fi);
     FF_CUDA(cudaGetLastError());
     if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
@@ -1130,6 +1143,15 @@ int ff_solve_passes(const ff_plan *p, size_t bytes, void *density, void *potenti
 int ff_plan_check(const ff_plan *p, void *stream) {
   if (!p) return set_error(FF_ERR_INVALID, "ff_plan_check: null plan");
   return take_device_status(p, static_cast<cudaStream_t>(stream));
+}
+
+int ff_plan_set_wait_limit(ff_plan *p, int iterations, int target_extra) {
+  if (!p) return set_error(FF_ERR_INVALID, "ff_plan_set_wait_limit: null plan");
+  if (iterations < 0 || target_extra < 0)
+    return set_error(FF_ERR_INVALID, "ff_plan_set_wait_limit: negative argument");
+  p->wait_iters = iterations;
+  p->dep_extra = target_extra;
+  return FF_OK;
 }
 
 int ff_plan_destroy(ff_plan *p) {

@@ -19,6 +19,7 @@ template <typename T> struct PassArgs {
   double dd[3];            // wavenumber scales (ParisPencil.cpp:9-11)
   int *status;             // device status word (kDev*), 0 = ok
   int l2_ahead;            // z passes: block b prefetches block b + l2_ahead's input into L2 (0: off)
+  int wait_iters;          // iteration limit of the first wait for an inbound copy (0: built-in)
 };
 
 constexpr int kZThreads = 256;
@@ -54,17 +55,21 @@ struct ZTileIO {
   uint64_t *mbar;      // TMAIO: barrier of the inbound copy
   uint32_t parity;     // TMAIO: its phase
   int *status;         // TMAIO: timeout report
+  int wait_iters;      // TMAIO: iteration limit of the wait (0: built-in)
 };
 
 // Inbound bulk copy of `bytes` (rounded up to 16) from src into dst, waited
-// for on every thread with an iteration limit.
+// for on every thread with an iteration limit.  On a timeout the status word
+// is set and thread 0 waits again, with the built-in limit, for the copy in
+// flight to land before the block may leave (its shared memory is the copy's
+// destination).
 __device__ __forceinline__ bool bulk_in(void *dst, const void *src, size_t bytes, const ZTileIO &io) {
   if (threadIdx.x == 0) {
     const uint32_t b = (uint32_t)((bytes + 15) & ~size_t(15));
     mbar_expect_tx(io.mbar, b);
     bulk_load(dst, src, b, io.mbar);
   }
-  const bool ok = mbar_wait_bounded(io.mbar, io.parity);
+  const bool ok = mbar_wait_bounded(io.mbar, io.parity, io.wait_iters);
   if (__syncthreads_or(!ok)) {
     if (threadIdx.x == 0) {
       atomicExch(io.status, kDevTmaTimeout);
@@ -406,7 +411,7 @@ __device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T
 // (fence_proxy_async_smem) and barriered before the call.
 template <typename C, int W, bool XPASS>
 __device__ __forceinline__ bool tma_tile(const CUtensorMap *tmap, C *sm, uint64_t *mb, uint32_t parity, int n,
-                                         int box_rows, int o, int kt, int *status) {
+                                         int box_rows, int o, int kt, int *status, int wait_iters = 0) {
   if (threadIdx.x == 0) {
     mbar_expect_tx(mb, (uint32_t)(n * W * sizeof(C)));
     for (int q = 0; q < n / box_rows; q++) {
@@ -414,7 +419,7 @@ __device__ __forceinline__ bool tma_tile(const CUtensorMap *tmap, C *sm, uint64_
       else tma_load_3d(sm + q * box_rows * W, tmap, 2 * W * kt, q * box_rows, o, mb);
     }
   }
-  const bool ok = mbar_wait_bounded(mb, parity);
+  const bool ok = mbar_wait_bounded(mb, parity, wait_iters);
   if (__syncthreads_or(!ok)) {
     // report, and give the copy in flight a bounded chance to land before the
     // block's shared memory is released

@@ -123,6 +123,19 @@ int ff_solve_passes(const ff_plan *plan, size_t bytes, void *density, void *pote
  * is invalid.  ff_solve with `times` runs this check itself. */
 int ff_plan_check(const ff_plan *plan, void *stream);
 
+/* Test hook for the bounded device waits (no counterpart in the reference,
+ * whose CHECK prints and exits, gpu.hpp:69-87, and whose kernels never wait
+ * on one another).  iterations: iteration limit of the first wait of every
+ * inbound tile copy and of every dependency wait of the fused passes
+ * (FF_PASSES=3) in this plan's later solves; 0 restores the built-in limits
+ * (about a second each).  target_extra: added to the producer count that each
+ * dependency wait of the fused passes waits for (0 normally; 1 makes every
+ * such wait run out, so a test can check that the kernels return and that
+ * ff_plan_check reports FF_ERR_TIMEOUT).  A block whose wait ran out skips
+ * its tile (after waiting, with the built-in limit, for its own copy in
+ * flight), so that solve's result is invalid. */
+int ff_plan_set_wait_limit(ff_plan *plan, int iterations, int target_extra);
+
 int ff_plan_destroy(ff_plan *plan);
 
 /* ---- Batched form (no counterpart in the reference, which solves one grid
@@ -216,13 +229,14 @@ int ff_server_create(const ff_server_config *cfg, ff_server **server);
  * FF_ERR_NOMEM if the request alone exceeds the budget. */
 int ff_server_submit(ff_server *server, const int n[3], int precision, const void *f, int f_on_host, uint64_t *id);
 
-/* Waits up to timeout_ms (< 0: without limit) for the request; FF_OK when
- * its result is ready, FF_ERR_TIMEOUT otherwise.  info may be NULL. */
+/* Waits up to timeout_ms (negative, NaN or above 1e12: without limit) for the
+ * request; FF_OK when its result is ready, FF_ERR_TIMEOUT otherwise.  info may
+ * be NULL. */
 int ff_server_wait(ff_server *server, uint64_t id, double timeout_ms, ff_request_info *info);
 
 /* Completion queue: the id (and timings) of the next request that finished
  * and has not been returned by this call before, waiting up to timeout_ms
- * (< 0: without limit); FF_ERR_TIMEOUT if none.  A finished request keeps
+ * (negative, NaN or above 1e12: without limit); FF_ERR_TIMEOUT if none.  A finished request keeps
  * its buffers until fetched or released, so a client that waits for
  * requests in submission order can hold the budget with finished work while
  * an earlier, larger request waits for memory; taking completions from this
@@ -230,7 +244,9 @@ int ff_server_wait(ff_server *server, uint64_t id, double timeout_ms, ff_request
 int ff_server_next(ff_server *server, double timeout_ms, uint64_t *id, ff_request_info *info);
 
 /* Copies a finished request's potential (ni*nj*nk values) to phi (host or
- * device; phi NULL copies nothing) and releases the request's buffers. */
+ * device; phi NULL copies nothing) and releases the request's buffers.  While
+ * the copy runs the request is claimed: a fetch or release of the same id from
+ * another thread returns FF_ERR_INVALID, and the buffers are not reused. */
 int ff_server_fetch(ff_server *server, uint64_t id, void *phi, int phi_on_host);
 
 /* Releases a finished (or not yet admitted) request without copying. */
@@ -258,7 +274,8 @@ int ff_init_field(const int n[3], const double xlo[3], const double dx[3], int n
  * (FishFry.hpp:57-101), accumulated in FP64 with a fixed-order (deterministic)
  * two-stage reduction.  phi == NULL gives the phi = 0 pass that the reference
  * uses for its relative-norm scales (FishFry.hpp:146-159).  sums is HOST
- * memory; the call waits for the stream. */
+ * memory; the call waits for the stream, which must belong to the current
+ * device (as every stream passed to this library must). */
 int ff_error_sums(const int n[3], const double xlo[3], const double dx[3], int nmodes,
                   const ff_mode *modes, int precision, const void *phi, double sums[3], void *stream);
 
@@ -269,13 +286,16 @@ int ff_error_sums(const int n[3], const double xlo[3], const double dx[3], int n
  * loop, or they are plug-ins that may not call the CUDA allocator at all.
  * This entry point calls no cudaMalloc/cudaFree: its partial sums live in a
  * fixed device array inside the library (about 384 KB per GPU, held until the
- * process exits), so grids are limited to 2^30 points (1024^3); larger ones
+ * process exits), and grids are limited to 2^30 points (1024^3); larger ones
  * return FF_ERR_UNSUPPORTED.  Same arguments and results as ff_error_sums,
  * summed in a different fixed order (so sums agree to rounding, max exactly).
- * The first call on each device looks up that array's device address; make it
- * before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU (other streams, other threads) race and must be
- * serialised by the caller.  sums is HOST memory; the call waits for stream. */
+ * The first call on each device looks up that array's device address and
+ * remembers it; make that call before any stream capture, and do not use this
+ * entry point after a cudaDeviceReset in the same process (the remembered
+ * address is then stale).  The stream must belong to the current device.  All
+ * calls share the one array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller.  sums is HOST
+ * memory; the call waits for stream. */
 int ff_error_sums_noalloc(const int n[3], const double xlo[3], const double dx[3], int nmodes,
                           const ff_mode *modes, int precision, const void *phi, double sums[3], void *stream);
 

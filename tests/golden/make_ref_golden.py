@@ -77,4 +77,6 @@ def main(out, only=None):
 
 if __name__ == "__main__":
     sel = [tuple(int(x) for x in a.split("x")) for a in sys.argv[2:]]
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"), sel or None)
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_ref_golden.py OUT_DIR [NIxNJxNK ...]")
+    main(sys.argv[1], sel or None)

@@ -74,3 +74,7 @@ def test_reference_arm_line_on_rank_0_small_grid():
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+    # the same config dict as the repo arm's line for the same grid and GPU count
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["config"] == bench.solve_config((32, 32, 32), "fp64", 1)

@@ -218,15 +218,32 @@ def test_full_size_fp64(torch_cuda, ff, oracle, n):
 @pytest.mark.slow
 def test_full_size_fp32_1024(torch_cuda, ff):
     """1024^3 FP32 precision form with 64 random modes: relative L2 against the
-    analytic solution (the oracle is too slow at this size; the analytic phi
-    is exact to round-off for the alias-free modes)."""
+    FP64 solve of the same f (the FP64 path is itself pinned to the oracle at
+    1e-12 on the other sizes; the OpenMP oracle is too slow here), and against
+    the analytic solution (exact to round-off for the alias-free modes)."""
+    torch = torch_cuda
     n = (1024, 1024, 1024)
+    N = n[0] * n[1] * n[2]
     modes = ff.modes_generate(12345, 64, 32, ff.alias_free_kaxis(n))
+    plan64 = ff.Plan(n)
+    d = torch.empty(plan64.nbytes // 8, dtype=torch.float64, device="cuda")
+    p64 = torch.empty_like(d)
+    ff.init_field(n, d, modes, ff.FF_FP64)
+    f32 = d[:N].float()          # the FP32 solve sees f rounded once to FP32
+    d[:N].copy_(f32.double())    # and the FP64 solve the same values
+    plan64.solve(d, p64)
+    phi64 = p64[:N].clone()
+    del d, p64
+    plan64.close()
     plan = ff.Plan(n, precision=ff.FF_FP32)
-    d = torch_cuda.empty(plan.nbytes // 4, dtype=torch_cuda.float32, device="cuda")
-    p = torch_cuda.empty_like(d)
-    ff.init_field(n, d, modes, ff.FF_FP32)
+    d = torch.empty(plan.nbytes // 4, dtype=torch.float32, device="cuda")
+    p = torch.empty_like(d)
+    d[:N].copy_(f32)
+    del f32
     plan.solve(d, p)
+    phi32 = p[:N].double()
+    rel = float(torch.linalg.vector_norm(phi32 - phi64) / torch.linalg.vector_norm(phi64))
+    assert rel <= FP32_TOL, rel
     s0 = ff.error_sums(n, None, modes, ff.FF_FP32)
     s1 = ff.error_sums(n, p, modes, ff.FF_FP32)
     assert (s1[1] / s0[1]) ** 0.5 <= FP32_TOL
@@ -254,6 +271,37 @@ def test_parity_with_reference_binary(torch_cuda, ff, n, tmp_path):
     plan.solve(d, p)
     phi = p[:N].cpu().numpy().reshape(n)
     assert rel_l2(phi, phi_ref) <= FP64_TOL
+
+
+# The reference's own harness (main.cpp, FishFry.hpp, gpu.hpp, TimeStamp.hpp,
+# unchanged) compiled against include/ParisPencil.hpp and libfishfry.so by
+# oracle/ref/Makefile: the drop-in boundary exercised by the code it replaces.
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "fishfry_dropin")
+RUN_RE = re.compile(r"^(\d+): Time (\S+) Rate (\S+) L_1 (\S+) L_2 (\S+) L_\\inf (\S+)", re.M)
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN), reason="drop-in harness not built (oracle/ref/Makefile)")
+@pytest.mark.parametrize("n", [(64, 64, 64), (256, 256, 256)])
+def test_reference_harness_drives_dropin(ff, n):
+    r = subprocess.run([DROPIN, "1", "1", "1", *map(str, n), "3"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = r.stdout
+    assert re.search(r"FishFry<\w*ParisPencil>: %dx%dx%d points over 1x1x1 MPI processes" % n, out), out
+    runs = RUN_RE.findall(out)
+    assert [int(x[0]) for x in runs] == [0, 1, 2, 3], out
+    golden = open(os.path.join(ROOT, "tests", "golden", "ref_printout_%dx%dx%d.txt" % n)).read()
+    want = [float(x) for x in RUN_RE.findall(golden)[1][3:]]
+    for run in runs:
+        t, rate = float(run[1]), float(run[2])
+        assert t > 0 and abs(rate * t / (n[0] * n[1] * n[2]) - 1) < 1e-3
+        got = [float(x) for x in run[3:]]
+        # the reference's own diff kernel and norms on this build's phi: round-off, as the reference's phi
+        for g, w in zip(got, want):
+            assert abs(g - w) <= 1e-14, (got, want)
+    # the phase table: the reference's table code over this build's stamps
+    assert "Times Averaged across Iterations" in out
+    for name in ["Total"] + ff.phase_names(ff.Plan(n)):
+        assert re.search(r"\(\s*[\d.]+%\) \| " + re.escape(name) + "$", out, re.M), name
 
 
 @pytest.mark.parametrize("n", [(64, 64, 64), (30, 45, 50), (512, 16, 24), (16, 512, 512)])

@@ -46,6 +46,24 @@ def test_noalloc_sums_match_allocating_entry_point(torch_cuda, ff):
         assert got[2] == want[2], (call, got, want)
 
 
+def test_noalloc_sums_match_oracle(torch_cuda, ff, oracle):
+    """The same sums from the CPU oracle's restatement of the reference's diff
+    kernel (FishFry.hpp:57-101), for two fields in a row and for the phi = 0
+    pass.  The fields are O(1) away from the analytic phi, so the last-bit
+    differences between the device's and the host's sin/cos/exp stay far below
+    the tolerance."""
+    torch = torch_cuda
+    rng = np.random.default_rng(11)
+    for n in [(64, 48, 40), (37, 20, 11)]:
+        for call in range(2):
+            phi = rng.standard_normal(n) * (call + 1)
+            got = noalloc_sums(ff, n, torch.from_numpy(phi.ravel()).cuda())
+            want = oracle.diff_sums(phi)
+            assert np.allclose(got, want, rtol=RTOL, atol=0), (n, call, got, want)
+        z = noalloc_sums(ff, n, None)
+        assert np.allclose(z, oracle.diff_sums(np.zeros(n)), rtol=RTOL, atol=0), (n, z)
+
+
 def test_noalloc_scale_pass_and_fp32(torch_cuda, ff):
     torch = torch_cuda
     n = (64, 48, 40)
