@@ -34,6 +34,8 @@ EXPORTS = [
     "ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_next", "ff_server_fetch",
     "ff_server_release",
     "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy",
+    "ff_slab_create", "ff_slab_layout", "ff_slab_forward", "ff_slab_xpass", "ff_slab_backward", "ff_slab_check",
+    "ff_slab_destroy",
 ]
 
 
@@ -117,6 +119,16 @@ def _declare(L):
     L.ff_server_check.argtypes = [vp]
     L.ff_server_reset_stats.argtypes = [vp]
     L.ff_server_destroy.argtypes = [vp]
+    L.ff_slab_create.argtypes = [i3, d3, d3, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+    L.ff_slab_layout.argtypes = [vp, i3, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
+    L.ff_slab_forward.argtypes = [vp, vp, vp, ctypes.POINTER(vp), vp]
+    L.ff_slab_xpass.argtypes = [vp, vp, ctypes.POINTER(vp), vp]
+    L.ff_slab_backward.argtypes = [vp, vp, vp, vp, vp]
+    L.ff_slab_check.argtypes = [vp, vp]
+    L.ff_slab_destroy.argtypes = [vp]
+    for name in ("ff_slab_create", "ff_slab_layout", "ff_slab_forward", "ff_slab_xpass", "ff_slab_backward",
+                 "ff_slab_check", "ff_slab_destroy"):
+        getattr(L, name).restype = ctypes.c_int
     for name in ("ff_server_create", "ff_server_submit", "ff_server_wait", "ff_server_next", "ff_server_fetch",
                  "ff_server_release",
                  "ff_server_stats", "ff_server_reset_stats", "ff_server_check", "ff_server_destroy"):

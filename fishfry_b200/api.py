@@ -293,6 +293,24 @@ class ParisPencil:
             stamps.append((name, max(t, t1) if q + 1 == len(ms) else t))
 
 
+def init_field_at(n, xlo, dx, f, modes=None, precision=FF_FP64, stream=None):
+    """f on the device for the n points x = xlo + i*dx (per axis): one rank's
+    block of the harness's field (FishFry.hpp:22-44, :137-139)."""
+    nm, mp, keep = modes_array(modes)
+    check(lib().ff_init_field(int3(n), dbl3(xlo), dbl3(dx), nm, mp, int(precision), _ptr(f), _stream(stream)),
+          "ff_init_field")
+
+
+def error_sums_at(n, xlo, dx, phi, modes=None, precision=FF_FP64, stream=None):
+    """{sum|d|, sum d^2, max|d|} over the n points x = xlo + i*dx (one rank's
+    block; FishFry.hpp:57-101)."""
+    nm, mp, keep = modes_array(modes)
+    out = (ctypes.c_double * 3)()
+    check(lib().ff_error_sums(int3(n), dbl3(xlo), dbl3(dx), nm, mp, int(precision), _ptr(phi), out,
+                              _stream(stream)), "ff_error_sums")
+    return [out[0], out[1], out[2]]
+
+
 def init_field(n, f, modes=None, precision=FF_FP64, stream=None):
     """f on the device: analytic right-hand side (FishFry.hpp:22-44) + modes."""
     _, _, xlo, dx = reference_domain(n)

@@ -21,8 +21,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-pthread", "-I" + INCLUDE]
 
 LIB_SOURCES = ["ff_solve.cu", "ff_bluestein.cu", "ff_field.cu", "ff_batch.cu", "ff_batch_f64.cu", "ff_batch_f32.cu",
-               "ff_serve.cu"]
-HEADERS = ["ff_fft.cuh", "ff_tiles.cuh", "ff_status.hpp", "ff_batch.hpp", "ff_batch_dev.cuh", "ff_bluestein.hpp"]
+               "ff_serve.cu", "ff_slab.cu"]
+HEADERS = ["ff_fft.cuh", "ff_tiles.cuh", "ff_status.hpp", "ff_batch.hpp", "ff_batch_dev.cuh", "ff_bluestein.hpp",
+           "ff_plan.hpp"]
 
 
 def _nvcc():

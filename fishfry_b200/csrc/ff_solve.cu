@@ -29,8 +29,9 @@
 
 #include "ff_bluestein.hpp"
 #include "ff_fft.cuh"
-#include "ff_tiles.cuh"
+#include "ff_plan.hpp"
 #include "ff_status.hpp"
+#include "ff_tiles.cuh"
 
 namespace ff {
 
@@ -229,25 +230,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kZThreads, 3)
   constexpr int S = plan_stages(H);
   constexpr int RF = plan_radix(H, S - 1);
   const int j = o;
-  const int ni = a.ni;
   const double jd = double(min(j, a.nj - j)) * a.dd[1];
-  const double j2 = jd * jd;
-  const double ddi = a.dd[0], ddk = a.dd[2];
-  const double minvN = -a.invN;
-  // d = -1/((i2 + j2) + k2) as ParisPencil.cpp:276-279 forms it, times 1/N
-  auto filt = [&](int pos, int c, C v) -> C {
-    const int kx = r + 2 * rev_ct<H>(pos);
-    const int kh = kh0 + c;
-    if (c >= ncol) return v;
-    if ((kx | j | kh) == 0) return mk((T)0, (T)0);
-    const double id = double(min(kx, ni - kx)) * ddi;
-    const double kd = double(kh) * ddk;
-    const double d = recip_pos((id * id + j2) + kd * kd) * minvN;
-    return cscale(v, (T)d);
-  };
+  const XFilter flt{a.ni, j, kh0, ncol, jd * jd, a.dd[0], a.dd[2], -a.invN};
+  // block r's H-point position p holds frequency r + 2*rev_H(p); over a last
+  // DIF group the H-point frequency steps by H/RF, the full one by 2*H/RF
+  auto k0_of = [r](int base) { return r + 2 * rev_ct<H>(base); };
   if (ok) {
     dif_ct<H, S - 1, 0, false, Map::ColFast, W, NT, false, (sizeof(T) == 8), 2>(ax, tile_, tile_, tile_, W);
-    fused_filter_stage<RF, W, NT, H, C>(H, tile_, tile_, filt);
+    x_filter_stage<RF, W, NT, H, C>(H, tile_, tile_, flt, k0_of, 2 * (H / RF));
     __syncthreads();
     dit_ct<H, S - 2, true, Map::ColFast, W, NT, (sizeof(T) == 8), 2>(ax, tile_, tile_, W);
   }
@@ -453,63 +443,6 @@ __global__ void k_wavenumbers(int n, int count, int folded, double dd, double *k
 
 // ====================================================================== plan
 using namespace ff;
-
-namespace ff {
-
-// Launch shape of a strided pass (one TMA tile per block).
-struct StridedCfg {
-  int N;          // specialised length of the kernel, 0 = runtime plan
-  int W;          // columns per tile
-  int box_rows;   // rows per TMA box (a divisor of n, at most 256)
-  size_t smem;    // dynamic shared memory: one tile + alignment slack
-  int grid;       // one block per tile
-};
-
-// Launch shape of a fused persistent pass.
-struct FusedCfg {
-  int NZ, NY;     // specialised z and y lengths of the kernel (0 = runtime plan)
-  size_t smem;
-  int grid;
-  int lag;
-  int prod_pp, cons_pp;
-};
-
-}  // namespace ff
-
-struct ff_plan {
-  int n[3];
-  int precision;
-  int nh, nhp;
-  double dd[3];
-  size_t bytes;
-  int device;
-  int num_sms;
-  void *dmem;
-  AxisDev<double2> axd[3];
-  AxisDev<float2> axf[3];
-  double *kk[3];
-  int *status;
-  int *counters;       // fused passes: 2 tickets + 2 x ni plane counts
-  int fused;           // 1: three launches (fused z/y passes), 0: five launches
-  int zN;              // z passes: specialised length, 0 = runtime plan
-  bool zbulk;          // z passes: line blocks by bulk copies
-  int zW, zP;          // z passes: line pairs per block, line pitch in complex values
-  size_t zsmem;
-  unsigned ztiles;
-  int l2_ahead;        // forward z pass: L2 prefetch distance in blocks (0: off)
-  int wait_iters;      // bounded device waits: iteration limit of the first wait (0: built-in)
-  int dep_extra;       // fused passes: added to every dependency wait's target (test hook, 0)
-  StridedCfg ycfg, xcfg;
-  FusedCfg fwd, inv;
-  // axes with a prime factor above 7: padded convolution length M (0 for a
-  // 2^a 3^b 5^c 7^d axis), their tables, and the launch shape of each pass kind
-  // (0 z fwd, 1 y fwd, 2 x, 3 y inv, 4 z inv) that transforms such an axis
-  int bsM[3];
-  BsAxis<double2> bsd[3];
-  BsAxis<float2> bsf[3];
-  BsCfg bscfg[5];
-  cudaEvent_t ev[FF_MAX_PHASES + 1];
-};
 
 namespace ff {
 
@@ -791,26 +724,6 @@ template <typename T> static int spectrum_map(const ff_plan *p, void *base, cons
   return encode_spectrum_map(base, p->n[0], p->n[1], p->nh, p->nhp, sizeof(T), cfg.W, cfg.box_rows, xpass, map);
 }
 
-template <typename T> static PassArgs<T> pass_args(const ff_plan *p) {
-  PassArgs<T> a;
-  a.ni = p->n[0];
-  a.nj = p->n[1];
-  a.nk = p->n[2];
-  a.nh = p->nh;
-  a.nhp = p->nhp;
-  for (int d = 0; d < 3; d++) {
-    if constexpr (sizeof(T) == 8) a.ax[d] = p->axd[d];
-    else a.ax[d] = p->axf[d];
-    a.kk[d] = p->kk[d];
-  }
-  a.invN = 1.0 / (double(p->n[0]) * double(p->n[1]) * double(p->n[2]));
-  for (int d = 0; d < 3; d++) a.dd[d] = p->dd[d];
-  a.status = p->status;
-  a.l2_ahead = p->l2_ahead;
-  a.wait_iters = p->wait_iters;
-  return a;
-}
-
 template <typename T>
 static int launch_solve(const ff_plan *p, void *density, void *potential, cudaStream_t st, bool timed,
                         int npass = 5) {
@@ -897,11 +810,44 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
   return FF_OK;
 }
 
+int allow_dyn_smem_fn(const void *fn, size_t *avail) {
+  cudaFuncAttributes fa;
+  FF_CUDA(cudaFuncGetAttributes(&fa, fn));
+  const size_t lim = kMaxDynSmem - fa.sharedSizeBytes;
+  FF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim));
+  if (avail) *avail = lim;
+  return FF_OK;
+}
+
+template <typename T> static int launch_z(const ff_plan *p, bool inverse, void *in, void *out, cudaStream_t st) {
+  using C = typename Cplx<T>::type;
+  const PassArgs<T> a = pass_args<T>(p);
+  if (p->bsM[2]) {
+    const BsAxis<C> *bs;
+    if constexpr (sizeof(T) == 8) bs = &p->bsd[2];
+    else bs = &p->bsf[2];
+    return bs_launch<T>(inverse ? 4 : 0, in, out, a, *bs, p->bscfg[inverse ? 4 : 0], st);
+  }
+  if (!inverse)
+    zfwd_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(static_cast<const T *>(in),
+                                                                          static_cast<C *>(out), a, p->zW, p->zP);
+  else
+    zinv_kernel<T>(p->zN, p->zbulk)<<<p->ztiles, kZThreads, p->zsmem, st>>>(static_cast<const C *>(in),
+                                                                          static_cast<T *>(out), a, p->zW, p->zP);
+  FF_CUDA(cudaGetLastError());
+  return FF_OK;
+}
+
+int plan_launch_z(const ff_plan *p, bool inverse, void *in, void *out, cudaStream_t st) {
+  return p->precision == FF_FP64 ? launch_z<double>(p, inverse, in, out, st)
+                                 : launch_z<float>(p, inverse, in, out, st);
+}
+
 static int plan_phases(const ff_plan *p) { return p->fused ? 3 : 5; }
 
 // Reads and clears the device status word; FF_ERR_TIMEOUT if a bounded wait
 // inside a kernel gave up.
-static int take_device_status(const ff_plan *p, cudaStream_t st) {
+int take_device_status(const ff_plan *p, cudaStream_t st) {
   int h = 0;
   FF_CUDA(cudaMemcpyAsync(&h, p->status, sizeof(int), cudaMemcpyDeviceToHost, st));
   FF_CUDA(cudaStreamSynchronize(st));

@@ -299,14 +299,73 @@ __device__ __forceinline__ void fused_filter_stage(int n_rt, LD &ld, ST &st, FL 
   }
 }
 
+// Parameters of the x pass's filter on one tile (plane j, columns kh0 ..
+// kh0 + ncol - 1): d = -1/N / ((i2 + j2) + k2) with i2 = (min(kx, ni - kx)*ddi)^2,
+// j2 = (min(j, nj - j)*ddj)^2 and k2 = (kh*ddk)^2, as ParisPencil.cpp:270-284
+// forms them (summed in that order), and 0 at the zero mode.
+struct XFilter {
+  int ni, j, kh0, ncol;
+  double j2, ddi, ddk, minvN;
+};
+
 // 1/x for x > 0 by two Newton-Raphson steps y <- y + y*(1 - x*y) from the
-// single-precision reciprocal (about 2^-23 -> 2^-46 -> full double).
+// hardware's approximate FP64 reciprocal (rcp.approx.ftz.f64; each step
+// squares the relative error, so the seed's error of at most about 2^-20
+// ends below double rounding).  The seed needs no conversions to and from
+// FP32, which ran on the same narrow conversion pipe as the seed itself.
 __device__ __forceinline__ double recip_pos(double x) {
-  double y = (double)__frcp_rn((float)x);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
   double e = fma(-x, y, 1.0);
   y = fma(y, e, y);
   e = fma(-x, y, 1.0);
   return fma(y, e, y);
+}
+
+// The last DIF stage of the x forward transform, the filter and the first
+// DIT stage of the inverse on one register group of R positions base + r of
+// an n-point tile.  Their frequencies are k0 + r*kstep with k0 = k0_of(base)
+// (the last DIF stage's digit is the slowest digit of the frequency; kstep is
+// n/R, or the full line's step when the tile is half of a longer line), so
+// the filter needs one frequency lookup per group; the column's k2 is formed
+// once per group.
+template <int R, int W, int NT, int NC, typename C, typename LD, typename ST, typename K0>
+__device__ __forceinline__ void x_filter_stage(int n_rt, LD &ld, ST &st, const XFilter &f, const K0 &k0_of,
+                                               int kstep) {
+  using T = typename Real<C>::type;
+  const int n = NC ? NC : n_rt;
+  const int step = kstep;
+  auto body = [&](int it) {
+    const int c = it % W;
+    const int base = (it / W) * R;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = ld(base + r, c);
+    Dft<R, false, C>::run(v);
+    const int kh = f.kh0 + c;
+    const double kd = double(kh) * f.ddk;
+    const double k2 = kd * kd;
+    const int k0 = k0_of(base);
+    const bool live = c < f.ncol;
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const int kx = k0 + r * step;
+      const double id = double(min(kx, f.ni - kx)) * f.ddi;
+      double d = recip_pos((id * id + f.j2) + k2) * f.minvN;
+      if ((kx | f.j | kh) == 0) d = 0.0;
+      if (live) v[r] = cscale(v[r], (T)d);
+    }
+    Dft<R, true, C>::run(v);
+#pragma unroll
+    for (int r = 0; r < R; r++) st(base + r, c, v[r]);
+  };
+  if constexpr (NC > 0 && (W * (NC / R)) % NT == 0) {
+    constexpr int ITER = W * (NC / R) / NT;
+#pragma unroll
+    for (int q = 0; q < ITER; q++) body((int)threadIdx.x + q * NT);
+  } else {
+    for (int it = threadIdx.x; it < W * (n / R); it += NT) body(it);
+  }
 }
 
 __device__ __forceinline__ unsigned char *align128(unsigned char *p) {
@@ -319,31 +378,42 @@ __device__ __forceinline__ unsigned char *align128(unsigned char *p) {
 // (plane j, rows i).
 
 // y transform of one tile; stage 0 reads through ld0 (the TMA-filled tile or
-// HBM/L2 directly), the last stage stores from registers straight to HBM at
-// the digit-reversed rows.
-template <typename T, int W, bool INV, int N, typename LD0>
-__device__ __forceinline__ void y_tile(LD0 &ld0, typename Cplx<T>::type *dst, const PassArgs<T> &a, int o, int kt,
-                                       typename Cplx<T>::type *sm) {
+// HBM/L2 directly), the last stage stores from registers straight to HBM:
+// frequency row j of the tile's columns goes to row_at(j)[0 .. ncol-1].
+template <typename T, int W, bool INV, int N, typename LD0, typename RowAt>
+__device__ __forceinline__ void y_tile_rows(LD0 &ld0, const RowAt &row_at, const PassArgs<T> &a, int kt,
+                                            typename Cplx<T>::type *sm) {
   using C = typename Cplx<T>::type;
   const AxisDev<C> &ax = a.ax[1];
-  const int kh0 = kt * W;
-  const int ncol = min(W, a.nh - kh0);
-  const long base = (long)o * a.nj * a.nhp + kh0;
-  const int pitch = a.nhp;
+  const int ncol = min(W, a.nh - kt * W);
   const auto rl = rev_last<N>(ax);
   PointTile<W, C> tile{sm};
   auto gst = [&](int pos, int c, C v) {
-    if (c < ncol) dst[base + (long)rl(pos) * pitch + c] = v;
+    if (c < ncol) row_at(rl(pos))[c] = v;
   };
   dif_all<N, INV, Map::ColFast, W, kZThreads, false, (sizeof(T) == 8)>(ax, ld0, tile, gst, W);
 }
 
-// x transform of one TMA-filled tile: forward, filter, inverse.  The inverse
-// ends in natural order in place, so the finished tile leaves by TMA stores
-// of the same boxes it came in with (columns past nh are clipped).
-template <typename T, int W, int N>
-__device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T> &a, int j, int kt, int box_rows,
+// y transform of one tile of plane o, stored into the spectrum dst at the
+// same plane and columns.
+template <typename T, int W, bool INV, int N, typename LD0>
+__device__ __forceinline__ void y_tile(LD0 &ld0, typename Cplx<T>::type *dst, const PassArgs<T> &a, int o, int kt,
                                        typename Cplx<T>::type *sm) {
+  using C = typename Cplx<T>::type;
+  C *base = dst + (long)o * a.nj * a.nhp + kt * W;
+  const int pitch = a.nhp;
+  auto row_at = [base, pitch](int j) { return base + (long)j * pitch; };
+  y_tile_rows<T, W, INV, N>(ld0, row_at, a, kt, sm);
+}
+
+// x transform of one tile in shared memory (plane j of the x pencils,
+// columns kt*W ..): forward, filter, inverse.  The filter takes the global
+// row jf of an njf-row grid (the plane itself on one GPU).  The last stage
+// writes natural order through gst: back into the tile (gst = the tile) or
+// straight to HBM.
+template <typename T, int W, int N, typename GST>
+__device__ __forceinline__ void x_tile_core(const PassArgs<T> &a, int jf, int njf, int kt,
+                                            typename Cplx<T>::type *sm, GST &gst) {
   using C = typename Cplx<T>::type;
   constexpr int NT = kZThreads;
   // FP64: twiddle powers by recurrence (fewer table loads); FP32: table loads
@@ -353,48 +423,46 @@ __device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T
   const int n = N > 0 ? N : ax.n;
   const int kh0 = kt * W;
   const int ncol = min(W, a.nh - kh0);
-  const auto rl = rev_last<N>(ax);
   PointTile<W, C> tile{sm};
-  PointTile<W, C> &gst = tile;
-  // d = -1/((i2 + j2) + k2) with i2 = (min(i, ni-i)*ddi)^2 etc., as
-  // ParisPencil.cpp:276-279 forms it, times 1/N
-  const int ni = a.ni;
-  const double jd = double(min(j, a.nj - j)) * a.dd[1];
-  const double j2 = jd * jd;
-  const double ddi = a.dd[0], ddk = a.dd[2];
-  const double minvN = -a.invN;
-  auto filt = [&](int pos, int c, C v) -> C {
-    const int kx = rl(pos);
-    const int kh = kh0 + c;
-    if (c >= ncol) return v;
-    if ((kx | j | kh) == 0) return mk((T)0, (T)0);
-    const double id = double(min(kx, ni - kx)) * ddi;
-    const double kd = double(kh) * ddk;
-    const double d = recip_pos((id * id + j2) + kd * kd) * minvN;
-    return cscale(v, (T)d);
-  };
+  const double jd = double(min(jf, njf - jf)) * a.dd[1];
+  const XFilter flt{a.ni, jf, kh0, ncol, jd * jd, a.dd[0], a.dd[2], -a.invN};
   if constexpr (N > 0) {
     constexpr int S = plan_stages(N);
     constexpr int RF = plan_radix(N, S - 1);
+    auto k0_of = [](int base) { return rev_ct<N>(base); };
     if constexpr (S > 1) {
       dif_ct<N, S - 1, 0, false, Map::ColFast, W, NT, false, TWX>(ax, tile, tile, tile, W);
-      fused_filter_stage<RF, W, NT, N, C>(N, tile, tile, filt);
+      x_filter_stage<RF, W, NT, N, C>(N, tile, tile, flt, k0_of, N / RF);
       __syncthreads();
       dit_ct<N, S - 2, true, Map::ColFast, W, NT, TWX>(ax, tile, gst, W);
     } else {
-      fused_filter_stage<RF, W, NT, N, C>(N, tile, gst, filt);
+      x_filter_stage<RF, W, NT, N, C>(N, tile, gst, flt, k0_of, N / RF);
     }
   } else {
     const int S = ax.nstages;
     if (S > 1) dif_rt<false, Map::ColFast, W, NT, false, TWX>(ax, S - 1, tile, tile, tile, W);
+    const int *rev = ax.rev;
+    auto k0_of = [rev](int base) { return __ldg(rev + base); };
     with_radix(ax.radix[S - 1], [&](auto tag) {
       constexpr int R = decltype(tag)::value;
-      if (S == 1) fused_filter_stage<R, W, NT, 0, C>(n, tile, gst, filt);
-      else fused_filter_stage<R, W, NT, 0, C>(n, tile, tile, filt);
+      if (S == 1) x_filter_stage<R, W, NT, 0, C>(n, tile, gst, flt, k0_of, n / R);
+      else x_filter_stage<R, W, NT, 0, C>(n, tile, tile, flt, k0_of, n / R);
     });
     __syncthreads();
     if (S > 1) dit_rt<true, Map::ColFast, W, NT, TWX>(ax, S - 2, tile, gst, W);
   }
+}
+
+// x transform of one TMA-filled tile: forward, filter, inverse.  The inverse
+// ends in natural order in place, so the finished tile leaves by TMA stores
+// of the same boxes it came in with (columns past nh are clipped).
+template <typename T, int W, int N>
+__device__ __forceinline__ void x_tile(const CUtensorMap *tmap, const PassArgs<T> &a, int j, int kt, int box_rows,
+                                       typename Cplx<T>::type *sm) {
+  using C = typename Cplx<T>::type;
+  const int n = N > 0 ? N : a.ax[0].n;
+  PointTile<W, C> tile{sm};
+  x_tile_core<T, W, N>(a, j, a.nj, kt, sm, tile);
   fence_proxy_async_smem();
   __syncthreads();
   if (threadIdx.x == 0) {

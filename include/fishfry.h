@@ -264,6 +264,57 @@ int ff_server_check(ff_server *server);
 /* Stops the loop (requests still queued are dropped) and frees everything. */
 int ff_server_destroy(ff_server *server);
 
+/* ---- Multi-rank solve over an x-slab decomposition: the reference's task
+ * grid (P, 1, 1) (ParisPencil.cpp:23-75 with mi = P, mj = mk = 1), one rank
+ * per GPU.  Rank r holds planes [r*di, r*di + planes) of the real field,
+ * di = ceil(n0/P) (ParisPencil.cpp:54); for the x pencils rank p holds rows
+ * [p*djp, p*djp + rows) of the spectrum with every x, djp = ceil(n1/P)
+ * (ParisPencil.cpp:61).  A solve is three device phases and two exchanges of
+ * equal blocks of di x djp x nhp complex values (the reference's
+ * MPI_Alltoall over its commI, ParisPencil.cpp:236, :312; nhp = n2/2+1 FP64,
+ * that rounded up to even FP32); the block from rank r to rank p holds r's
+ * planes and p's rows, [i - r*di][j - p*djp][kh].  The z and y transforms of
+ * the reference's other pencil exchanges are local here.  Lengths must be
+ * 2^a 3^b 5^c 7^d, at most FF_MAX_AXIS, with n0 and n1 at least P. */
+typedef struct ff_slab ff_slab;
+
+/* Rank `rank` of `nranks` (<= 64) for the grid n on the bounds lo/hi. */
+int ff_slab_create(const int n[3], const double lo[3], const double hi[3], int precision, int nranks, int rank,
+                   ff_slab **slab);
+
+/* layout[0..7] = {P, rank, di, djp, first_plane, planes, first_row, rows};
+ * *bytes = bytes each of density and potential must hold (the slab's real
+ * field or spectrum, or P blocks); *block_bytes = bytes of one block.  Any
+ * output may be NULL. */
+int ff_slab_layout(const ff_slab *slab, int layout[8], size_t *bytes, size_t *block_bytes);
+
+/* Phase 1 ("Real-to-complex FFT in Z", "Forward FFT in Y"): density holds the
+ * rank's planes of f (x slowest) and is destroyed; the z pass writes the
+ * slab's spectrum to potential, and the y pass stores the values of rank p's
+ * rows into the block at dst[p] (p < P, device pointers, 16-byte aligned):
+ * the caller's send buffer, or the block's place in rank p's receive buffer
+ * if the caller can store into it (peer memory).  Enqueued on stream. */
+int ff_slab_forward(const ff_slab *slab, void *density, void *potential, void *const *dst, void *stream);
+
+/* Phase 2 ("X FFTs and filter"): pencils holds the P blocks this rank
+ * received, rank 0's first (so [i][j - first_row][kh] for every i); x
+ * forward, filter (global wavenumbers, 1/N of the whole grid), x inverse;
+ * the values of rank q's planes go to the block at dst[q].  pencils is not
+ * written. */
+int ff_slab_xpass(const ff_slab *slab, const void *pencils, void *const *dst, void *stream);
+
+/* Phase 3 ("Backward FFT in Y", "Complex-to-real FFT in Z"): packed holds
+ * the P blocks this rank received back, rank 0's first; the y inverse writes
+ * the slab's spectrum to density, the z pass writes phi for the rank's planes
+ * to potential.  packed may be potential (it is read before the z pass
+ * writes), not density. */
+int ff_slab_backward(const ff_slab *slab, const void *packed, void *density, void *potential, void *stream);
+
+/* As ff_plan_check, for the slab's kernels. */
+int ff_slab_check(const ff_slab *slab, void *stream);
+
+int ff_slab_destroy(ff_slab *slab);
+
 /* Harness: write f on the device at x = xlo + i*dx (FishFry.hpp:22-44),
  * plus sum_m a_m cos(k_m.x + theta_m) for the given modes (nmodes may be 0).
  * precision selects a double or float field.  Enqueued on stream. */
