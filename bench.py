@@ -266,6 +266,35 @@ def solve_config(n, precision, world):
             "l2": "inputs larger than L2 (%.2f GB per field > 126 MB)" % (N * esz / 1e9)}
 
 
+def reference_binary_on_gpu(n=(256, 256, 256), runs=10):
+    """The reference itself on this GPU: its own ParisPencil.cpp + main.cpp with
+    cuFFT (oracle/_ref/fishfry_ref, built from the reference's sources with a
+    one-rank MPI stub), and this build's driver with the same arguments; both
+    print the reference harness's per-run Time (host wall time of a solve,
+    FishFry.hpp:198).  256^3 is the largest cube the reference launches on one
+    GPU.  Returns None where the reference binary was not built."""
+    import re
+    ref = os.path.join(ROOT, "oracle", "_ref", "fishfry_ref")
+    ours = os.path.join(ROOT, "fishfry_b200", "bin", "fishfry")
+    if not (os.path.exists(ref) and os.path.exists(ours)):
+        return None
+    args = ["1", "1", "1"] + [str(x) for x in n] + [str(runs)]
+    out = {}
+    for name, exe in (("reference", ref), ("fishfry_b200", ours)):
+        r = subprocess.run([exe] + args, capture_output=True, text=True, timeout=300)
+        if r.returncode != 0:
+            return {"error": "%s exited %d: %s" % (name, r.returncode, r.stderr[-200:])}
+        times = [float(m.group(2)) for m in re.finditer(r"^(\d+): Time (\S+)", r.stdout, re.M) if m.group(1) != "0"]
+        l2 = re.search(r"L_2 (\S+)", r.stdout)
+        out[name] = {"ms_per_solve": 1e3 * statistics.median(times), "runs": len(times),
+                     "rel_l2_vs_analytic": float(l2.group(1)) if l2 else None}
+    out["grid"] = list(n)
+    out["speedup"] = out["reference"]["ms_per_solve"] / out["fishfry_b200"]["ms_per_solve"]
+    out["what"] = ("median per-run Time of the reference harness's printout (host wall time of one solve), "
+                   "the reference with cuFFT vs this build, same arguments, same GPU")
+    return out
+
+
 def run_reference(args):
     """The reference's algorithm on the host cores: each step one oracle
     solve (ParisPencil's FFT solve restated in C++/OpenMP) of a sample grid
@@ -454,6 +483,12 @@ def run_ours(args):
                                               "what": "scipy.fft rfftn, -1/k^2, irfftn (pocketfft), one solve"}
             except Exception as e:   # a missing scipy does not cost the line
                 cpu["scipy_fft_yardstick"] = {"unavailable": str(e)[:120]}
+            try:
+                rg = reference_binary_on_gpu()
+                if rg is not None:
+                    cpu["reference_binary_on_gpu"] = rg
+            except Exception as e:
+                cpu["reference_binary_on_gpu"] = {"error": str(e)[:200]}
         line = {
             "metric": "512^3 FP64 solve points/s", "value": value, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,

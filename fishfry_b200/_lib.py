@@ -21,7 +21,7 @@ FF_ERR_TASKS = 7
 FF_FP64 = 0
 FF_FP32 = 1
 FF_MAX_PHASES = 5
-FF_MAX_AXIS = 1800
+FF_MAX_AXIS = 4096
 
 # Every symbol include/fishfry.h declares.
 EXPORTS = [

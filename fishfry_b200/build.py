@@ -51,21 +51,26 @@ def _run(cmd, verbose):
 
 def build_lib(verbose=False, force=False):
     srcs = [os.path.join(CSRC, s) for s in LIB_SOURCES]
-    deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "fishfry.h")]
-    if not force and not _stale(LIB, deps):
+    shared = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "fishfry.h"), os.path.abspath(__file__)]
+    objdir = os.path.join(HERE, "lib", "obj")
+    os.makedirs(objdir, exist_ok=True)
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+    # a translation unit is rebuilt when it, a shared header or this recipe is newer than its object
+    todo = [(s, o) for s, o in zip(srcs, objs) if force or _stale(o, [s] + shared)]
+    if not todo and not _stale(LIB, objs):
         return LIB
-    os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    objs = [os.path.join(HERE, "lib", os.path.basename(s) + ".o") for s in srcs]
-    # translation units compile in parallel (each is one nvcc process)
+    # translation units compile in parallel (each is one nvcc process); each
+    # object is written under a temporary name and renamed when complete
     from concurrent.futures import ThreadPoolExecutor
-    with ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as ex:
-        for f in [ex.submit(_run, [_nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o], verbose) for s, o in zip(srcs, objs)]:
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 1))) as ex:
+        futs = [ex.submit(_run, [_nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o + ".tmp"], verbose) for s, o in todo]
+        for f in futs:
             f.result()
+    for _, o in todo:
+        os.replace(o + ".tmp", o)
     tmp = LIB + ".tmp"
     _run([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-lpthread"], verbose)
     os.replace(tmp, LIB)
-    for o in objs:
-        os.remove(o)
     return LIB
 
 

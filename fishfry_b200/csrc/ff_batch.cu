@@ -71,6 +71,16 @@ struct ff_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t ev[6] = {};
+  // Grids the batch kernels cannot hold (an axis with a prime factor above 7,
+  // or longer than their tiles) are solved by their own single-grid plans
+  // (Bluestein passes where needed) after the batched launches, on the same
+  // stream.  where[u] of caller index u: >= 0 the index among the batched
+  // grids, < 0 side grid -where[u]-1.
+  int user_count = 0;
+  std::vector<int> where;
+  std::vector<ff_plan *> side;
+  std::vector<size_t> side_bytes;
+  cudaEvent_t side_ev[2] = {};
 };
 
 namespace ff {
@@ -457,26 +467,16 @@ int time_pass(ff_batch *b, int kind, cudaStream_t st, int reps, float *ms) {
 
 extern "C" {
 
-int ff_batch_create(int count, const int *dims, const double *lo, const double *hi, int precision, ff_batch **out) {
-  if (!out) return set_error(FF_ERR_INVALID, "ff_batch_create: null output");
-  *out = nullptr;
-  if (count < 1 || !dims) return set_error(FF_ERR_INVALID, "ff_batch_create: count %d or dims missing", count);
-  if (precision != FF_FP64 && precision != FF_FP32)
-    return set_error(FF_ERR_INVALID, "ff_batch_create: precision %d is neither FF_FP64 nor FF_FP32", precision);
-  for (int g = 0; g < count; g++) {
-    const int rc = batch_check_dims(dims + 3 * g, lo ? lo + 3 * g : nullptr, hi ? hi + 3 * g : nullptr,
-                                    "ff_batch_create", g);
-    if (rc != FF_OK) return rc;
-  }
-  ff_batch *b = new ff_batch();
+}  // extern "C"
+
+namespace ff {
+namespace {
+
+// The batched grids' tables, descriptors, work lists and events (count >= 1
+// grids that batch_check_dims accepted).  On failure the caller destroys b.
+int batch_create_core(ff_batch *b, int count, const int *dims, const double *lo, const double *hi,
+                      int precision) {
   b->count = count;
-  b->precision = precision;
-  b->csz = precision == FF_FP64 ? 16 : 8;
-  if (cudaGetDevice(&b->device) != cudaSuccess ||
-      cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess) {
-    delete b;
-    return set_error(FF_ERR_CUDA, "ff_batch_create: no current CUDA device");
-  }
   b->desc_size = desc_size(precision);
   // distinct axis lengths -> one table set each
   std::map<int, size_t> table_of;
@@ -499,15 +499,12 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
   b->dmem_size = off;
   if (cudaMalloc(&b->dmem, off) != cudaSuccess) {
     cudaGetLastError();
-    delete b;
+    b->dmem = nullptr;
     return set_error(FF_ERR_NOMEM, "ff_batch_create: cudaMalloc(%zu) for tables failed", off);
   }
   if (cudaMallocHost((void **)&b->desc_host, (size_t)count * b->desc_size) != cudaSuccess ||
       cudaMallocHost((void **)&b->maps_host, (size_t)count * 2 * sizeof(CUtensorMap)) != cudaSuccess) {
     cudaGetLastError();
-    if (b->desc_host) cudaFreeHost(b->desc_host);
-    cudaFree(b->dmem);
-    delete b;
     return set_error(FF_ERR_NOMEM, "ff_batch_create: pinned descriptor image");
   }
   char *base = static_cast<char *>(b->dmem);
@@ -547,8 +544,88 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
     for (int k = 0; k < 5; k++) h.shape[k] = batch_shape_for(precision, h, k);
   }
   if (rc == FF_OK) rc = build_work(b);
+  return rc;
+}
+
+// A grid the batch kernels take: every axis 2^a 3^b 5^c 7^d and short enough
+// for their tiles (batch_check_dims).
+bool batchable(const int n[3]) {
+  for (int d = 0; d < 3; d++)
+    if (!smooth2357(n[d]) || (size_t)n[d] * 128 + 128 > kBatchSmem) return false;
+  return true;
+}
+
+}  // namespace
+}  // namespace ff
+
+extern "C" {
+
+int ff_batch_create(int count, const int *dims, const double *lo, const double *hi, int precision, ff_batch **out) {
+  if (!out) return set_error(FF_ERR_INVALID, "ff_batch_create: null output");
+  *out = nullptr;
+  if (count < 1 || !dims) return set_error(FF_ERR_INVALID, "ff_batch_create: count %d or dims missing", count);
+  if (precision != FF_FP64 && precision != FF_FP32)
+    return set_error(FF_ERR_INVALID, "ff_batch_create: precision %d is neither FF_FP64 nor FF_FP32", precision);
+  std::vector<int> bdims;
+  std::vector<double> blo, bhi;
+  for (int g = 0; g < count; g++) {
+    const int *n = dims + 3 * g;
+    for (int d = 0; d < 3; d++) {
+      if (n[d] < 1) return set_error(FF_ERR_INVALID, "ff_batch_create: grid %d n[%d] = %d < 1", g, d, n[d]);
+      if (n[d] > FF_MAX_AXIS)
+        return set_error(FF_ERR_UNSUPPORTED, "ff_batch_create: grid %d n[%d] = %d is above %d", g, d, n[d],
+                         FF_MAX_AXIS);
+      if (lo && hi && n[d] > 1 && !(hi[3 * g + d] > lo[3 * g + d]))
+        return set_error(FF_ERR_INVALID, "ff_batch_create: grid %d hi[%d] <= lo[%d]", g, d, d);
+    }
+  }
+  ff_batch *b = new ff_batch();
+  b->user_count = count;
+  b->precision = precision;
+  b->csz = precision == FF_FP64 ? 16 : 8;
+  if (cudaGetDevice(&b->device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device) != cudaSuccess) {
+    delete b;
+    return set_error(FF_ERR_CUDA, "ff_batch_create: no current CUDA device");
+  }
+  int rc = FF_OK;
+  b->where.resize(count);
+  for (int g = 0; g < count && rc == FF_OK; g++) {
+    const int *n = dims + 3 * g;
+    if (batchable(n)) {
+      b->where[g] = (int)(bdims.size() / 3);
+      for (int d = 0; d < 3; d++) {
+        bdims.push_back(n[d]);
+        if (lo && hi) {
+          blo.push_back(lo[3 * g + d]);
+          bhi.push_back(hi[3 * g + d]);
+        }
+      }
+    } else {
+      // the reference domain of the grid unless bounds are given
+      double glo[3], ghi[3];
+      for (int d = 0; d < 3; d++) {
+        glo[d] = lo && hi ? lo[3 * g + d] : -M_PI;
+        ghi[d] = lo && hi ? hi[3 * g + d] : M_PI - 2.0 * M_PI / n[d];
+      }
+      ff_plan *pl = nullptr;
+      rc = ff_plan_create(n, glo, ghi, precision, &pl);
+      if (rc != FF_OK) break;
+      size_t nb = 0;
+      ff_plan_bytes(pl, &nb);
+      b->where[g] = -(int)b->side.size() - 1;
+      b->side.push_back(pl);
+      b->side_bytes.push_back(nb);
+    }
+  }
+  const int nb = (int)(bdims.size() / 3);
+  if (rc == FF_OK && nb > 0)
+    rc = batch_create_core(b, nb, bdims.data(), lo && hi ? blo.data() : nullptr, lo && hi ? bhi.data() : nullptr,
+                           precision);
   for (int e = 0; e < 6 && rc == FF_OK; e++)
     if (cudaEventCreate(&b->ev[e]) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_create: event");
+  for (int e = 0; e < 2 && rc == FF_OK; e++)
+    if (cudaEventCreate(&b->side_ev[e]) != cudaSuccess) rc = set_error(FF_ERR_CUDA, "ff_batch_create: event");
   if (rc != FF_OK) {
     ff_batch_destroy(b);
     return rc;
@@ -559,56 +636,111 @@ int ff_batch_create(int count, const int *dims, const double *lo, const double *
 
 int ff_batch_bytes(const ff_batch *b, int index, size_t *bytes) {
   if (!b || !bytes) return set_error(FF_ERR_INVALID, "ff_batch_bytes: null argument");
-  if (index < 0 || index >= b->count) return set_error(FF_ERR_INVALID, "ff_batch_bytes: index %d", index);
-  *bytes = b->bytes[index];
+  if (index < 0 || index >= b->user_count) return set_error(FF_ERR_INVALID, "ff_batch_bytes: index %d", index);
+  const int w = b->where[index];
+  *bytes = w >= 0 ? b->bytes[w] : b->side_bytes[-w - 1];
   return FF_OK;
 }
 
 int ff_batch_shape(const ff_batch *b, int index, int kind, int *W, int *ct, int *tma) {
-  if (!b || index < 0 || index >= b->count || kind < 0 || kind > 4)
+  if (!b || index < 0 || index >= b->user_count || kind < 0 || kind > 4)
     return set_error(FF_ERR_INVALID, "ff_batch_shape: bad argument");
-  if (W) *W = b->grids[index].shape[kind].W;
-  if (ct) *ct = b->grids[index].shape[kind].ct;
-  if (tma) *tma = b->grids[index].shape[kind].tma;
+  const int w = b->where[index];
+  if (w < 0)
+    return set_error(FF_ERR_UNSUPPORTED, "ff_batch_shape: grid %d runs through its own single-grid plan", index);
+  if (W) *W = b->grids[w].shape[kind].W;
+  if (ct) *ct = b->grids[w].shape[kind].ct;
+  if (tma) *tma = b->grids[w].shape[kind].tma;
   return FF_OK;
 }
 
 int ff_batch_radices(const ff_batch *b, int index, int axis, int radix[16], int *count) {
-  if (!b || index < 0 || index >= b->count || axis < 0 || axis > 2 || !radix || !count)
+  if (!b || index < 0 || index >= b->user_count || axis < 0 || axis > 2 || !radix || !count)
     return set_error(FF_ERR_INVALID, "ff_batch_radices: bad argument");
-  const AxisDev<double2> &ax = b->grids[index].axd[axis];
+  if (b->where[index] < 0)
+    return set_error(FF_ERR_UNSUPPORTED, "ff_batch_radices: grid %d runs through its own single-grid plan", index);
+  const AxisDev<double2> &ax = b->grids[b->where[index]].axd[axis];
   *count = ax.nstages;
   for (int q = 0; q < ax.nstages; q++) radix[q] = ax.radix[q];
   return FF_OK;
 }
 
+}  // extern "C"
+
+namespace ff {
+namespace {
+
+// The caller's per-grid buffers split into the batched grids' arrays.
+int split_buffers(const ff_batch *b, void *const *density, void *const *potential, std::vector<void *> &bd,
+                  std::vector<void *> &bp) {
+  bd.assign(b->count, nullptr);
+  bp.assign(b->count, nullptr);
+  for (int u = 0; u < b->user_count; u++) {
+    if (!density[u] || !potential[u]) return set_error(FF_ERR_INVALID, "ff_batch: null buffer for grid %d", u);
+    if (b->where[u] >= 0) {
+      bd[b->where[u]] = density[u];
+      bp[b->where[u]] = potential[u];
+    }
+  }
+  return FF_OK;
+}
+
+int batch_status(ff_batch *b, cudaStream_t st) {
+  int rc = b->count > 0 ? take_status(b, st) : FF_OK;
+  for (ff_plan *pl : b->side) {
+    const int r2 = ff_plan_check(pl, st);
+    if (rc == FF_OK) rc = r2;
+  }
+  return rc;
+}
+
+}  // namespace
+}  // namespace ff
+
+extern "C" {
+
 int ff_batch_solve(ff_batch *b, void *const *density, void *const *potential, void *stream, ff_phase_times *times) {
   if (!b || !density || !potential) return set_error(FF_ERR_INVALID, "ff_batch_solve: null argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int rc = set_buffers(b, density, potential);
-  if (rc == FF_OK) rc = upload_desc(b, st);
-  if (rc == FF_OK && !b->exec) rc = capture(b);
+  std::vector<void *> bd, bp;
+  int rc = split_buffers(b, density, potential, bd, bp);
   if (rc != FF_OK) return rc;
-  FF_CUDA(cudaGraphLaunch(b->exec, st));
+  if (b->count > 0) {
+    rc = set_buffers(b, bd.data(), bp.data());
+    if (rc == FF_OK) rc = upload_desc(b, st);
+    if (rc == FF_OK && !b->exec) rc = capture(b);
+    if (rc != FF_OK) return rc;
+  }
+  if (times && b->count == 0) FF_CUDA(cudaEventRecord(b->side_ev[0], st));
+  if (b->count > 0) FF_CUDA(cudaGraphLaunch(b->exec, st));
+  for (int u = 0; u < b->user_count; u++) {
+    const int w = b->where[u];
+    if (w >= 0) continue;
+    rc = ff_solve(b->side[-w - 1], b->side_bytes[-w - 1], density[u], potential[u], stream, nullptr);
+    if (rc != FF_OK) return rc;
+  }
   if (times) {
-    FF_CUDA(cudaEventSynchronize(b->ev[5]));
+    FF_CUDA(cudaEventRecord(b->side_ev[1], st));
+    FF_CUDA(cudaEventSynchronize(b->side_ev[1]));
+    // per pass: the batched grids' five launches (zero if none); total: the
+    // whole solve, single-grid plans of the other grids included
     times->count = 5;
     for (int k = 0; k < 5; k++) {
       float ms = 0;
-      FF_CUDA(cudaEventElapsedTime(&ms, b->ev[k], b->ev[k + 1]));
+      if (b->count > 0) FF_CUDA(cudaEventElapsedTime(&ms, b->ev[k], b->ev[k + 1]));
       times->ms[k] = ms;
     }
     float tot = 0;
-    FF_CUDA(cudaEventElapsedTime(&tot, b->ev[0], b->ev[5]));
+    FF_CUDA(cudaEventElapsedTime(&tot, b->count > 0 ? b->ev[0] : b->side_ev[0], b->side_ev[1]));
     times->total_ms = tot;
-    return take_status(b, st);
+    return batch_status(b, st);
   }
   return FF_OK;
 }
 
 int ff_batch_check(ff_batch *b, void *stream) {
   if (!b) return set_error(FF_ERR_INVALID, "ff_batch_check: null batch");
-  return take_status(b, static_cast<cudaStream_t>(stream));
+  return batch_status(b, static_cast<cudaStream_t>(stream));
 }
 
 // Coordinate search over tile shapes: for each pass and each axis length
@@ -618,11 +750,16 @@ int ff_batch_check(ff_batch *b, void *stream) {
 // W in {d/2, d, 2d} around the default d line pairs, strided passes 1, 2 or
 // 4 rows of 128 bytes per tile row; each with the compile-time tile (where
 // the length has one) and with the runtime plan.
-int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, void *stream, int reps) {
-  if (!b || !density || !potential) return set_error(FF_ERR_INVALID, "ff_batch_tune: null argument");
+int ff_batch_tune(ff_batch *b, void *const *density_u, void *const *potential_u, void *stream, int reps) {
+  if (!b || !density_u || !potential_u) return set_error(FF_ERR_INVALID, "ff_batch_tune: null argument");
   if (reps < 1) reps = 3;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int rc = set_buffers(b, density, potential);
+  std::vector<void *> bd, bp;   // the batched grids' buffers (grids with own plans are not tuned)
+  int rc = split_buffers(b, density_u, potential_u, bd, bp);
+  if (rc != FF_OK || b->count == 0) return rc;
+  void *const *density = bd.data();
+  void *const *potential = bp.data();
+  rc = set_buffers(b, density, potential);
   if (rc != FF_OK) return rc;
   for (int g = 0; g < b->count; g++) {
     FF_CUDA(cudaMemsetAsync(density[g], 0, b->bytes[g], st));
@@ -704,6 +841,9 @@ int ff_batch_tune(ff_batch *b, void *const *density, void *const *potential, voi
 int ff_batch_destroy(ff_batch *b) {
   if (!b) return FF_OK;
   drop_graph(b);
+  for (ff_plan *pl : b->side) ff_plan_destroy(pl);
+  for (int e = 0; e < 2; e++)
+    if (b->side_ev[e]) cudaEventDestroy(b->side_ev[e]);
   for (int e = 0; e < 6; e++)
     if (b->ev[e]) cudaEventDestroy(b->ev[e]);
   if (b->cap) cudaStreamDestroy(b->cap);

@@ -546,7 +546,16 @@ template <typename T, int N> static StridedKernel<T> strided_n(int kind) {
   return kind == 0 ? k_strided<T, W, false, false, N>
                    : kind == 1 ? k_strided<T, W, false, true, N> : k_strided<T, W, true, false, N>;
 }
-template <typename T> static StridedKernel<T> strided_kernel(int kind, int N) {
+// Narrower tiles for lines too long for 128-byte rows: 64- or 32-byte rows
+// (runtime plans only; every specialised length fits with 128-byte rows).
+template <typename T, int W> static StridedKernel<T> strided_narrow(int kind) {
+  return kind == 0 ? k_strided<T, W, false, false, 0>
+                   : kind == 1 ? k_strided<T, W, false, true, 0> : k_strided<T, W, true, false, 0>;
+}
+template <typename T> static StridedKernel<T> strided_kernel(int kind, int N, int W = 128 / (2 * (int)sizeof(T))) {
+  constexpr int WF = 128 / (2 * (int)sizeof(T));
+  if (W == WF / 2) return strided_narrow<T, WF / 2>(kind);
+  if (W == WF / 4) return strided_narrow<T, WF / 4>(kind);
   if (N == 1024)   // one tile per 2-block cluster
     return kind == 0 ? k_strided_pair<T, false, false, 1024>
                      : kind == 1 ? k_strided_pair<T, false, true, 1024> : k_strided_pair<T, true, false, 1024>;
@@ -618,28 +627,37 @@ template <typename T> static int configure(ff_plan *p) {
     if (rc == FF_OK) rc = allow_dyn_smem(zinv_kernel<T>(p->zN, p->zbulk), nullptr);
     if (rc != FF_OK) return rc;
   }
-  // strided tiles: W 128-byte columns x n rows, one per block
+  // strided tiles: W columns of 128-byte rows x n rows, one per block; lines
+  // too long for that (above about 1800 points FP64, 3600 FP32) take 64- or
+  // 32-byte rows, i.e. half or a quarter of the columns per tile
   const int W = 128 / (int)csz;
-  const int ktiles = (p->nh + W - 1) / W;
   for (int kind = 0; kind < 3; kind++) {
     StridedCfg &cfg = kind == 2 ? p->xcfg : p->ycfg;
     const int n = kind == 2 ? ni : nj;
     if (p->bsM[kind == 2 ? 0 : 1]) continue;
     cfg.N = special_n(n);
     cfg.W = W;
-    cfg.box_rows = largest_divisor_at_most(n, 256, 1);
     const int pair = cfg.N == 1024 ? 2 : 1;   // tile rows split over a 2-block cluster
-    cfg.smem = (size_t)(n / pair) * W * csz + 128;
+    while ((size_t)(n / pair) * cfg.W * csz + 1024 > kMaxDynSmem && cfg.W * csz > 32) {
+      cfg.W /= 2;
+      cfg.N = 0;
+    }
+    cfg.box_rows = largest_divisor_at_most(n, 256, 1);
+    cfg.smem = (size_t)(n / pair) * cfg.W * csz + 128;
     size_t avail = 0;
-    rc = allow_dyn_smem(strided_kernel<T>(kind, cfg.N), &avail);
+    rc = allow_dyn_smem(strided_kernel<T>(kind, cfg.N, cfg.W), &avail);
     if (rc != FF_OK) return rc;
     if (cfg.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "no tile shape for an axis of %d points", n);
-    cfg.grid = (kind == 2 ? nj : ni) * ktiles * pair;
+    cfg.grid = (kind == 2 ? nj : ni) * ((p->nh + cfg.W - 1) / cfg.W) * pair;
   }
+  const int ktiles = (p->nh + W - 1) / W;
+  // the fused passes hold a whole y tile of 128-byte rows per block (not with
+  // Bluestein axes, 1024-point y lines or narrowed tiles)
+  const bool can_fuse = !any_bs && p->ycfg.N != 1024 && p->ycfg.W == W && p->xcfg.W == W;
   // fused passes: persistent blocks over the in-order tile queue (not with
   // Bluestein axes)
   const int zpp = (nj + 2 * p->zW - 1) / (2 * p->zW);   // z tiles per plane (pairs never cross planes)
-  for (int dir = 0; dir < 2 && !any_bs; dir++) {
+  for (int dir = 0; dir < 2 && can_fuse; dir++) {
     FusedCfg &fc = dir == 0 ? p->fwd : p->inv;
     fused_pair(nk, nj, &fc.NZ, &fc.NY);
     fc.smem = std::max(p->zsmem, p->ycfg.smem);
@@ -676,8 +694,7 @@ template <typename T> static int configure(ff_plan *p) {
   const char *ahead = getenv("FF_L2_AHEAD");
   p->l2_ahead = ahead ? std::max(0, atoi(ahead)) : 3 * p->num_sms;
   const char *mode = getenv("FF_PASSES");
-  // the fused passes hold a whole y tile per block: not for 1024-point y lines
-  p->fused = mode && strcmp(mode, "3") == 0 && p->ycfg.N != 1024 && !any_bs;
+  p->fused = mode && strcmp(mode, "3") == 0 && can_fuse;
   return FF_OK;
 }
 
@@ -752,7 +769,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     fwd_kernel<T>(p->fwd.NZ, p->fwd.NY)<<<p->fwd.grid, kZThreads, p->fwd.smem, st>>>(D, Ps, a, ff);
     FF_CUDA(cudaGetLastError());
     if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
-    strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
+    strided_kernel<T>(2, p->xcfg.N, p->xcfg.W)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
     FF_CUDA(cudaGetLastError());
     if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
     FuseArgs fi{p->counters + 1, p->counters + 2 + ni, ni, p->inv.prod_pp, p->inv.cons_pp, p->inv.lag, p->zW, p->zP,
@@ -776,7 +793,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     rc = bs_launch<T>(1, Ps, Ps, a, bsax(1), p->bscfg[1], st);
     if (rc != FF_OK) return rc;
   } else {
-    strided_kernel<T>(0, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ps, a, p->ycfg.box_rows);
+    strided_kernel<T>(0, p->ycfg.N, p->ycfg.W)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ps, a, p->ycfg.box_rows);
     FF_CUDA(cudaGetLastError());
   }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
@@ -785,7 +802,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     rc = bs_launch<T>(2, Ps, Ps, a, bsax(0), p->bscfg[2], st);
     if (rc != FF_OK) return rc;
   } else {
-    strided_kernel<T>(2, p->xcfg.N)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
+    strided_kernel<T>(2, p->xcfg.N, p->xcfg.W)<<<p->xcfg.grid, kZThreads, p->xcfg.smem, st>>>(xmapP, Ps, a, p->xcfg.box_rows);
     FF_CUDA(cudaGetLastError());
   }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));
@@ -794,7 +811,7 @@ static int launch_solve(const ff_plan *p, void *density, void *potential, cudaSt
     rc = bs_launch<T>(3, Ps, Ds, a, bsax(1), p->bscfg[3], st);
     if (rc != FF_OK) return rc;
   } else {
-    strided_kernel<T>(1, p->ycfg.N)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ds, a, p->ycfg.box_rows);
+    strided_kernel<T>(1, p->ycfg.N, p->ycfg.W)<<<p->ycfg.grid, kZThreads, p->ycfg.smem, st>>>(ymapP, Ds, a, p->ycfg.box_rows);
     FF_CUDA(cudaGetLastError());
   }
   if (timed) FF_CUDA(cudaEventRecord(p->ev[ev++], st));

@@ -35,8 +35,8 @@ extern "C" {
 typedef enum {
   FF_OK = 0,
   FF_ERR_INVALID = 1,          /* bad argument (null pointer, non-positive size, ...) */
-  FF_ERR_UNSUPPORTED = 2,      /* length above FF_MAX_AXIS (or, in the batched and serving
-                                  forms, with a prime factor > 7) */
+  FF_ERR_UNSUPPORTED = 2,      /* length above FF_MAX_AXIS, or no tile shape fits (or, in the
+                                  batched and serving forms, above 574 points) */
   FF_ERR_BYTES = 3,            /* caller buffers smaller than ff_plan_bytes() */
   FF_ERR_CUDA = 4,             /* a CUDA runtime call failed (message has the name) */
   FF_ERR_NOMEM = 5,            /* device allocation failed */
@@ -46,8 +46,12 @@ typedef enum {
 
 enum { FF_FP64 = 0, FF_FP32 = 1 };
 
-/* Longest supported axis: the shared-memory tile holds one full line per column. */
-#define FF_MAX_AXIS 1800
+/* Longest axis a plan takes.  A strided-pass tile holds whole lines in shared
+ * memory: 128-byte rows (8 FP64 / 16 FP32 columns) up to about 1800 / 3600
+ * points, narrower rows (64 or 32 bytes) for longer lines.  A length with a
+ * prime factor above 7 also needs its Bluestein convolution length M >= 2n-1
+ * to fit: up to about 3600 points on x and y (FF_ERR_UNSUPPORTED beyond). */
+#define FF_MAX_AXIS 4096
 
 typedef struct ff_plan ff_plan;
 
@@ -78,7 +82,8 @@ typedef struct {
  * transformed by Bluestein's algorithm through an M-point convolution, M the
  * smallest 2^a 3^b 5^c 7^d >= 2n-1: its passes run plain-load tiles and
  * cost several times a 2^a 3^b 5^c 7^d length's (radix 8, 4, 2, 5, 3 and 7
- * stages). */
+ * stages); if no tile of M rows fits in shared memory the plan returns
+ * FF_ERR_UNSUPPORTED. */
 int ff_plan_create(const int n[3], const double lo[3], const double hi[3], int precision, ff_plan **plan);
 
 /* Bytes each of density and potential must hold (the half spectrum
@@ -140,12 +145,16 @@ int ff_plan_destroy(ff_plan *plan);
 
 /* ---- Batched form (no counterpart in the reference, which solves one grid
  * per ParisPencil).  `count` independent grids, dims[3g..3g+2] = (ni, nj, nk)
- * of grid g, each axis 2^a 3^b 5^c 7^d and at most 574 points; lo/hi (3 per grid)
- * give the physical bounds as ParisPencil's constructor takes them
+ * of grid g, each axis at most FF_MAX_AXIS; lo/hi (3 per grid) give the
+ * physical bounds as ParisPencil's constructor takes them
  * (ParisPencil.hpp:23), or NULL for the reference's domain [-pi, pi - 2pi/n].
  * A solve of the batch runs the same five passes as ff_solve, each pass one
- * persistent kernel launch over the tiles of all grids, the five launches
- * captured once into a CUDA graph and replayed. */
+ * persistent kernel launch over the tiles of all grids whose axes are
+ * 2^a 3^b 5^c 7^d and at most 574 points, the five launches captured once
+ * into a CUDA graph and replayed.  Every other grid (an axis with a prime
+ * factor above 7, or longer than the batch tiles hold) is solved by its own
+ * single-grid plan (Bluestein passes where needed) after the batched
+ * launches, on the same stream. */
 typedef struct ff_batch ff_batch;
 
 int ff_batch_create(int count, const int *dims, const double *lo, const double *hi, int precision, ff_batch **batch);
@@ -156,7 +165,8 @@ int ff_batch_bytes(const ff_batch *batch, int index, size_t *bytes);
 /* Solves every grid: density[g] and potential[g] are device buffers of at
  * least ff_batch_bytes(g) bytes, 16-byte aligned; density is destroyed.
  * Asynchronous on `stream` unless `times` is non-NULL (then times->ms[0..4]
- * are the five passes over all grids).  The first solve, and any solve whose
+ * are the five batched passes, times->total_ms the whole solve including the
+ * grids solved by their own plans).  The first solve, and any solve whose
  * buffer pointers differ from the previous one, uploads the grid descriptors
  * and waits for `stream`; solves of one batch must not overlap each other. */
 int ff_batch_solve(ff_batch *batch, void *const *density, void *const *potential, void *stream,
@@ -171,7 +181,8 @@ int ff_batch_solve(ff_batch *batch, void *const *density, void *const *potential
  * densities after tuning.  reps: timed launches per candidate (median). */
 int ff_batch_tune(ff_batch *batch, void *const *density, void *const *potential, void *stream, int reps);
 
-/* The tile shape pass `kind` (0..4) of grid `index` uses: W (line pairs for
+/* The tile shape pass `kind` (0..4) of grid `index` uses (FF_ERR_UNSUPPORTED
+ * for a grid solved by its own plan): W (line pairs for
  * the z passes, columns for the strided ones), ct (1: compile-time plan) and
  * tma (strided passes: 1 = one-plane tiles loaded by TMA boxes, 0 = tiles of
  * the flattened column index read straight from HBM; z passes of runtime

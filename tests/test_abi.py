@@ -37,11 +37,12 @@ def test_version_and_status_strings(ff):
     assert L.ff_plan_phases(None) == 0
 
 
-# any length up to FF_MAX_AXIS plans (prime factors above 5 through the
-# Bluestein passes); longer axes and non-positive ones are refused
-@pytest.mark.parametrize("n,status", [((1801, 7, 8), "FF_ERR_UNSUPPORTED"), ((8, 8, 1801), "FF_ERR_UNSUPPORTED"),
+# lengths up to FF_MAX_AXIS plan (prime factors above 7 through the
+# Bluestein passes, where their convolution fits); longer axes and
+# non-positive ones are refused before any device call
+@pytest.mark.parametrize("n,status", [((4097, 7, 8), "FF_ERR_UNSUPPORTED"), ((8, 8, 4097), "FF_ERR_UNSUPPORTED"),
                                       ((0, 8, 8), "FF_ERR_INVALID"), ((8, -2, 8), "FF_ERR_INVALID"),
-                                      ((8, 8, 2048), "FF_ERR_UNSUPPORTED"), ((8, 8, 1801), "FF_ERR_UNSUPPORTED")])
+                                      ((8, 8, 8192), "FF_ERR_UNSUPPORTED"), ((8, 5000, 8), "FF_ERR_UNSUPPORTED")])
 def test_plan_rejects_bad_sizes_before_any_device_call(ff, n, status):
     with pytest.raises(ff.FFError) as e:
         ff.Plan(n)
@@ -95,9 +96,11 @@ def test_driver_arguments_checked_on_host(ff):
     assert r.returncode == 1
 
 
-@pytest.mark.parametrize("dims,status", [([], "FF_ERR_INVALID"), ([(8, 8, 11)], "FF_ERR_UNSUPPORTED"),
+# (lengths the batch kernels do not take, e.g. 11 or 576, are accepted and
+# solved by single-grid plans; see test_batch_gpu.py)
+@pytest.mark.parametrize("dims,status", [([], "FF_ERR_INVALID"), ([(8, 8, 4097)], "FF_ERR_UNSUPPORTED"),
                                          ([(8, 8, 8), (0, 4, 4)], "FF_ERR_INVALID"),
-                                         ([(576, 8, 8)], "FF_ERR_UNSUPPORTED"), ([(8, 11, 8)], "FF_ERR_UNSUPPORTED")])
+                                         ([(5000, 8, 8)], "FF_ERR_UNSUPPORTED"), ([(8, -1, 8)], "FF_ERR_INVALID")])
 def test_batch_rejects_bad_dims_before_any_device_call(ff, dims, status):
     with pytest.raises(ff.FFError) as e:
         ff.Batch(dims)

@@ -198,3 +198,36 @@ def test_batch_tma_tiles_for_long_lines(torch_cuda, ff, oracle):
     batch.solve(d, p)
     for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
         assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL, (g, dims[g])
+
+
+# Grids the batch kernels do not take (an axis with a prime factor above 7,
+# or longer than their tiles) are solved by their own single-grid plans in
+# the same ff_batch_solve.
+WITH_SIDE = [(32, 48, 64), (97, 40, 36), (80, 96, 128), (36, 101, 50), (27, 30, 127), (600, 8, 12), (64, 64, 64)]
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, FP32_TOL)])
+def test_batch_with_prime_and_long_axes(torch_cuda, ff, oracle, precision, tol):
+    batch = ff.Batch(WITH_SIDE, precision=precision)
+    d, p = make_buffers(torch_cuda, batch, precision)
+    batch.tune(d, p)   # tunes the batched grids only
+    fs = init_all(ff, batch, d, modes_for(ff, 3), precision)
+    ms, total = batch.solve(d, p, timed=True)
+    assert total > 0 and len(ms) == 5
+    batch.check()
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        assert rel_l2(phi, oracle.solve(f)) <= tol, (g, batch.dims[g])
+    with pytest.raises(ff.FFError) as e:
+        batch.shape(1, 0)
+    assert e.value.status == ff.FF_ERR_UNSUPPORTED
+    assert batch.shape(0, 0)[0] > 0
+
+
+def test_batch_of_only_side_grids(torch_cuda, ff, oracle):
+    dims = [(97, 8, 10), (11, 13, 17)]
+    batch = ff.Batch(dims)
+    d, p = make_buffers(torch_cuda, batch, 0)
+    fs = init_all(ff, batch, d, lambda n: None, 0)
+    batch.solve(d, p, timed=True)
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL, g

@@ -57,6 +57,34 @@ def test_fp64_parity_with_oracle(torch_cuda, ff, oracle, n):
     assert rel_l2(phi, ref) <= FP64_TOL
 
 
+# Axes longer than the 128-byte-row tiles hold (narrower strided tiles; one
+# line pair per z tile), and lengths with a prime factor above 7 beyond 1800
+# points (Bluestein convolutions of 4032 and 6048 points).
+LONG_AXES = [(2048, 64, 64), (64, 2048, 32), (4096, 16, 16), (16, 4096, 8), (16, 16, 4096), (2048, 8, 2048),
+             (2003, 8, 8), (8, 2003, 6), (6, 8, 2003), (3001, 4, 4)]
+
+
+@pytest.mark.parametrize("n", LONG_AXES)
+def test_long_axes_fp64_parity_with_oracle(torch_cuda, ff, oracle, n):
+    f, phi = run_solve(torch_cuda, ff, n)
+    assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL
+
+
+@pytest.mark.parametrize("n", [(4096, 16, 16), (16, 4096, 8), (16, 16, 4096), (2003, 8, 8)])
+def test_long_axes_fp32_parity_with_oracle(torch_cuda, ff, oracle, n):
+    modes = ff.modes_generate(5, 16, 16, ff.alias_free_kaxis(n))
+    f64 = oracle.init_f(n, modes)
+    plan = ff.Plan(n, precision=ff.FF_FP32)
+    d = torch_cuda.zeros(plan.nbytes // 4, dtype=torch_cuda.float32, device="cuda")
+    p = torch_cuda.empty_like(d)
+    ff.init_field(n, d, modes, ff.FF_FP32)
+    N = f64.size
+    f32 = d[:N].double().cpu().numpy().reshape(n)
+    plan.solve(d, p)
+    phi = p[:N].double().cpu().numpy().reshape(n)
+    assert rel_l2(phi, oracle.solve(f32)) <= FP32_TOL
+
+
 @pytest.mark.parametrize("n", [(16, 16, 16), (30, 45, 50), (64, 64, 64)])
 def test_fp64_parity_random_field(torch_cuda, ff, oracle, n):
     rng = np.random.default_rng(11)
