@@ -262,12 +262,17 @@ template <typename T, int W> StridedFn<T, W> strided_fn(int kind) {
   return kind == 1 ? k_bs_strided<T, W, 0> : kind == 2 ? k_bs_strided<T, W, 2> : k_bs_strided<T, W, 1>;
 }
 
+// Checks that a tile of `need` bytes fits and lets fn use all the dynamic
+// shared memory there is: the limit is a property of the kernel, shared by
+// every plan, so it is never lowered to one plan's need (a later plan with a
+// smaller tile would otherwise break an earlier plan's launches).
 template <typename F> int raise_smem(F fn, size_t need) {
   cudaFuncAttributes fa;
   FF_CUDA(cudaFuncGetAttributes(&fa, fn));
   if (need + fa.sharedSizeBytes > kBsMaxSmem)
     return set_error(FF_ERR_UNSUPPORTED, "Bluestein tile of %zu bytes does not fit in shared memory", need);
-  FF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need));
+  FF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(kBsMaxSmem - fa.sharedSizeBytes)));
   return FF_OK;
 }
 

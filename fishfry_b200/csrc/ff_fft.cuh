@@ -39,6 +39,14 @@ __device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y
 template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk(a.x + b.x, a.y + b.y); }
 template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk(a.x - b.x, a.y - b.y); }
 template <typename C, typename S> __device__ __forceinline__ C cscale(C a, S s) { return mk(a.x * s, a.y * s); }
+// FP32 complex values as packed pairs: one sm_100 two-wide instruction for
+// both components (a - b as the fused a + (-1)*b, exact like the plain
+// subtraction).  Each component rounds as the scalar operation does.
+template <> __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+template <> __device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 // a*b
 template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
   return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

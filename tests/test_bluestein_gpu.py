@@ -153,12 +153,16 @@ def test_matches_reference_golden(torch_cuda, ff, path):
         assert abs(np.linalg.norm(phi) - float(g["phi_l2"])) <= FP64_TOL * float(g["phi_l2"])
 
 
-def test_batch_rejects_primes_above_7(ff):
-    """The batched and serving forms take 2^a 3^b 5^c 7^d lengths (no
-    Bluestein passes there); the single-grid plan takes any length."""
+def test_server_rejects_primes_above_7(torch_cuda, ff):
+    """The serving form takes 2^a 3^b 5^c 7^d lengths only (its requests run in
+    the batch kernels); a batch accepts any length, solving such grids by
+    their own plans (tests/test_batch_gpu.py)."""
+    srv = ff.Server(1 << 30, max_active=4)
+    f = torch_cuda.zeros(8 * 8 * 11, dtype=torch_cuda.float64, device="cuda")
     with pytest.raises(ff.FFError) as e:
-        ff.Batch([(8, 8, 11)])
+        srv.submit((8, 8, 11), f, ff.FF_FP64)
     assert e.value.status == ff.FF_ERR_UNSUPPORTED
+    srv.close()
 
 
 def test_batch_and_server_radix7_lengths(torch_cuda, ff, oracle):
@@ -196,3 +200,22 @@ def test_batch_and_server_radix7_lengths(torch_cuda, ff, oracle):
             assert rel_l2(out.cpu().numpy().reshape(n), ref) <= FP64_TOL, n
     finally:
         srv.close()
+
+
+def test_plans_with_different_bluestein_tiles_coexist(torch_cuda, ff, oracle):
+    """Two plans whose Bluestein passes need different shared memory, the
+    larger one created first and solved after the smaller one was created
+    (a kernel's shared-memory limit is shared by every plan)."""
+    big, small = (1009, 4, 6), (11, 8, 8)
+    rng = np.random.default_rng(4)
+    fb = rng.standard_normal(big)
+    fs = rng.standard_normal(small)
+    pb = ff.Plan(big)
+    ps = ff.Plan(small)
+    for plan, f in ((pb, fb), (ps, fs), (pb, fb)):
+        d = torch_cuda.zeros(plan.nbytes // 8, dtype=torch_cuda.float64, device="cuda")
+        p = torch_cuda.empty_like(d)
+        d[:f.size] = torch_cuda.from_numpy(f.ravel()).cuda()
+        plan.solve(d, p)
+        phi = p[:f.size].cpu().numpy().reshape(f.shape)
+        assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL
