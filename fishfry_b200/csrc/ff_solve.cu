@@ -17,7 +17,6 @@
 // The reference's 12 reorder kernels and 6 MPI_Alltoall self-copies reduce to
 // the choice of row stride in passes 2-4.
 
-#include <cooperative_groups.h>
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -117,141 +116,6 @@ __global__ void __launch_bounds__(kZThreads, 3)
   } else {
     PointTile<W, C> tile{sm};
     y_tile<T, W, INV, N>(tile, dst, a, o, kt, sm);
-  }
-}
-
-// ------------------------------------------- long lines on a CTA pair
-// A strided tile of N = 2H rows (N = 1024) would need 128 KB of shared
-// memory and a whole SM.  Instead a 2-block cluster holds it, block r keeping
-// rows [r*H, r*H + H) (64 KB, 128-byte rows, three blocks per SM).  The plan
-// is radix 2 first: the span-N radix-2 stage pairs row j of block 0 with row
-// j of block 1 and runs over distributed shared memory; what is left on each
-// block is an independent H-point transform (the compile-time plan of H,
-// twiddles from the N table), whose output frequency is k = r + 2*rev_H(pos).
-// The x pass mirrors it: H-point stages, filter, H-point inverse stages, and
-// the span-N radix-2 DIT stage across the pair last.
-
-// Cross-block radix-2 stage of span 2H on rows j of `lo` (block 0) and `hi`
-// (block 1); block r takes j in [r*H/2, (r+1)*H/2), so every pair of
-// locations belongs to one item (read and written in place).
-// The items are taken in batches of B whose loads (half of them from the
-// partner block) are all issued before any store.
-template <bool INV, bool DIT, int W, int H, typename C>
-__device__ __forceinline__ void pair_stage(C *lo, C *hi, int r, const AxisDev<C> &ax) {
-  constexpr int ITEMS = W * (H / 2);
-  constexpr int Q = ITEMS / kZThreads;
-  constexpr int B = 4;
-  static_assert(ITEMS % kZThreads == 0 && Q % B == 0, "pair stage shape");
-#pragma unroll 1
-  for (int q0 = 0; q0 < Q; q0 += B) {
-    C v0[B], v1[B];
-    int at[B], jj[B];
-#pragma unroll
-    for (int b = 0; b < B; b++) {
-      const int it = (int)threadIdx.x + (q0 + b) * kZThreads;
-      const int c = it % W;
-      jj[b] = r * (H / 2) + it / W;
-      at[b] = jj[b] * W + c;
-      v0[b] = lo[at[b]];
-      v1[b] = hi[at[b]];
-    }
-#pragma unroll
-    for (int b = 0; b < B; b++) {
-      C v[2] = {v0[b], v1[b]};
-      if (DIT) {
-        if (jj[b]) v[1] = twmul<INV>(v[1], ax.tw, jj[b]);
-        Dft<2, INV, C>::run(v);
-      } else {
-        Dft<2, INV, C>::run(v);
-        if (jj[b]) v[1] = twmul<INV>(v[1], ax.tw, jj[b]);
-      }
-      lo[at[b]] = v[0];
-      hi[at[b]] = v[1];
-    }
-  }
-}
-
-template <typename T, bool XPASS, bool INV, int N>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kZThreads, 3)
-    k_strided_pair(const __grid_constant__ CUtensorMap tmap, typename Cplx<T>::type *dst, const PassArgs<T> a,
-                   int box_rows) {
-  using C = typename Cplx<T>::type;
-  namespace cg = cooperative_groups;
-  constexpr int W = 128 / sizeof(C);
-  constexpr int H = N / 2;
-  constexpr int NT = kZThreads;
-  extern __shared__ unsigned char smraw[];
-  __shared__ __align__(8) uint64_t mbar;
-  cg::cluster_group cl = cg::this_cluster();
-  const int r = (int)cl.block_rank();
-  C *sm = reinterpret_cast<C *>(align128(smraw));
-  const AxisDev<C> &ax = XPASS ? a.ax[0] : a.ax[1];
-  const int ktiles = (a.nh + W - 1) / W;
-  const int tile = blockIdx.x / 2;
-  const int o = tile / ktiles, kt = tile - o * ktiles;
-  if (threadIdx.x == 0) {
-    mbar_init(&mbar, 1);
-    mbar_init_fence();
-    mbar_expect_tx(&mbar, (uint32_t)(H * W * sizeof(C)));
-    for (int q = 0; q < H / box_rows; q++) {
-      if (XPASS) tma_load_3d(sm + q * box_rows * W, &tmap, 2 * W * kt, o, r * H + q * box_rows, &mbar);
-      else tma_load_3d(sm + q * box_rows * W, &tmap, 2 * W * kt, r * H + q * box_rows, o, &mbar);
-    }
-  }
-  __syncthreads();
-  bool ok = mbar_wait_bounded(&mbar, 0, a.wait_iters);
-  ok = !__syncthreads_or(!ok);
-  if (!ok && threadIdx.x == 0) {
-    // report; the block still takes part in every cluster barrier below (its
-    // partner must not wait forever), but skips the work
-    atomicExch(a.status, kDevTmaTimeout);
-    mbar_wait_bounded(&mbar, 0);
-  }
-  cl.sync();   // both halves resident
-  C *peer = cl.map_shared_rank(sm, r ^ 1);
-  C *lo = r == 0 ? sm : peer;
-  C *hi = r == 0 ? peer : sm;
-  if (ok) pair_stage<INV && !XPASS, false, W, H>(lo, hi, r, ax);
-  cl.sync();   // the rest is local to each block
-  const int kh0 = kt * W;
-  const int ncol = min(W, a.nh - kh0);
-  PointTile<W, C> tile_{sm};
-  if (!XPASS) {
-    if (ok) {
-      const long base = (long)o * a.nj * a.nhp + kh0;
-      const int pitch = a.nhp;
-      auto gst = [&](int pos, int c, C v) {
-        if (c < ncol) dst[base + (long)(r + 2 * rev_ct<H>(pos)) * pitch + c] = v;
-      };
-      dif_ct<H, plan_stages(H), 0, INV, Map::ColFast, W, NT, false, false, 2>(ax, tile_, tile_, gst, W);
-    }
-    return;
-  }
-  constexpr int S = plan_stages(H);
-  constexpr int RF = plan_radix(H, S - 1);
-  const int j = o;
-  const double jd = double(min(j, a.nj - j)) * a.dd[1];
-  const XFilter flt{a.ni, j, kh0, ncol, jd * jd, a.dd[0], a.dd[2], -a.invN};
-  // block r's H-point position p holds frequency r + 2*rev_H(p); over a last
-  // DIF group the H-point frequency steps by H/RF, the full one by 2*H/RF
-  auto k0_of = [r](int base) { return r + 2 * rev_ct<H>(base); };
-  if (ok) {
-    dif_ct<H, S - 1, 0, false, Map::ColFast, W, NT, false, (sizeof(T) == 8), 2>(ax, tile_, tile_, tile_, W);
-    x_filter_stage<RF, W, NT, H, C>(H, tile_, tile_, flt, k0_of, 2 * (H / RF));
-    __syncthreads();
-    dit_ct<H, S - 2, true, Map::ColFast, W, NT, (sizeof(T) == 8), 2>(ax, tile_, tile_, W);
-  }
-  cl.sync();
-  if (ok) pair_stage<true, true, W, H>(lo, hi, r, ax);
-  cl.sync();   // both halves final; no remote access after this
-  if (!ok) return;
-  fence_proxy_async_smem();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int q = 0; q < H / box_rows; q++)
-      tma_store_3d(&tmap, 2 * W * kt, j, r * H + q * box_rows, sm + q * box_rows * W);
-    bulk_commit();
-    bulk_wait_read();
   }
 }
 
@@ -540,33 +404,27 @@ template <typename T> static ZInvKernel<T> zinv_kernel(int N, bool bulk) {
 }
 
 // kind: 0 = y forward, 1 = y inverse, 2 = x (forward, filter, inverse);
-// 128-byte rows (W = 8 FP64 / 16 FP32).
-template <typename T, int N> static StridedKernel<T> strided_n(int kind) {
-  constexpr int W = 128 / (2 * (int)sizeof(T));
+// N: the compile-time plan (0: runtime plan); W: columns per tile row.
+template <typename T, int N, int W> static StridedKernel<T> strided_nw(int kind) {
   return kind == 0 ? k_strided<T, W, false, false, N>
                    : kind == 1 ? k_strided<T, W, false, true, N> : k_strided<T, W, true, false, N>;
 }
-// Narrower tiles for lines too long for 128-byte rows: 64- or 32-byte rows
-// (runtime plans only; every specialised length fits with 128-byte rows).
-template <typename T, int W> static StridedKernel<T> strided_narrow(int kind) {
-  return kind == 0 ? k_strided<T, W, false, false, 0>
-                   : kind == 1 ? k_strided<T, W, false, true, 0> : k_strided<T, W, true, false, 0>;
-}
+// Lengths with compile-time strided tiles of 128-byte rows; 1024-point lines
+// take 64-byte rows (a 64 KB tile, as a 512-point line's), longer lines than
+// 128-byte rows hold take 64- or 32-byte rows with runtime plans.
+#define FF_FOR_EACH_STRIDED_N(X) X(64) X(128) X(256) X(512)
 template <typename T> static StridedKernel<T> strided_kernel(int kind, int N, int W = 128 / (2 * (int)sizeof(T))) {
   constexpr int WF = 128 / (2 * (int)sizeof(T));
-  if (W == WF / 2) return strided_narrow<T, WF / 2>(kind);
-  if (W == WF / 4) return strided_narrow<T, WF / 4>(kind);
-  if (N == 1024)   // one tile per 2-block cluster
-    return kind == 0 ? k_strided_pair<T, false, false, 1024>
-                     : kind == 1 ? k_strided_pair<T, false, true, 1024> : k_strided_pair<T, true, false, 1024>;
-#define FF_CASE(NN) if (N == NN) return strided_n<T, NN>(kind);
-  FF_FOR_EACH_SPECIAL_N(FF_CASE)
+  if (W == WF / 2) return N == 1024 ? strided_nw<T, 1024, WF / 2>(kind) : strided_nw<T, 0, WF / 2>(kind);
+  if (W == WF / 4) return strided_nw<T, 0, WF / 4>(kind);
+#define FF_CASE(NN) if (N == NN) return strided_nw<T, NN, WF>(kind);
+  FF_FOR_EACH_STRIDED_N(FF_CASE)
 #undef FF_CASE
-  return strided_n<T, 0>(kind);
+  return strided_nw<T, 0, WF>(kind);
 }
 
 // (z, y) length pairs with specialised fused kernels; others use (0, 0).
-#define FF_FOR_EACH_FUSED_PAIR(X) X(512, 512) X(256, 512) X(256, 256) X(1024, 1024)
+#define FF_FOR_EACH_FUSED_PAIR(X) X(512, 512) X(256, 512) X(256, 256)
 
 static void fused_pair(int nk, int nj, int *NZ, int *NY) {
   *NZ = *NY = 0;
@@ -637,23 +495,27 @@ template <typename T> static int configure(ff_plan *p) {
     if (p->bsM[kind == 2 ? 0 : 1]) continue;
     cfg.N = special_n(n);
     cfg.W = W;
-    const int pair = cfg.N == 1024 ? 2 : 1;   // tile rows split over a 2-block cluster
-    while ((size_t)(n / pair) * cfg.W * csz + 1024 > kMaxDynSmem && cfg.W * csz > 32) {
+    // 1024-point lines: 64-byte rows, so the tile stays 64 KB and three blocks
+    // share an SM (0.63 ms for the 1024x512x256 FP64 x pass, against 0.88 ms
+    // for a 1024-row tile split over a 2-block cluster and 1.06 ms for one
+    // block of 128-byte rows per SM)
+    if (cfg.N == 1024) cfg.W = W / 2;
+    while ((size_t)n * cfg.W * csz + 1024 > kMaxDynSmem && cfg.W * csz > 32) {
       cfg.W /= 2;
       cfg.N = 0;
     }
     cfg.box_rows = largest_divisor_at_most(n, 256, 1);
-    cfg.smem = (size_t)(n / pair) * cfg.W * csz + 128;
+    cfg.smem = (size_t)n * cfg.W * csz + 128;
     size_t avail = 0;
     rc = allow_dyn_smem(strided_kernel<T>(kind, cfg.N, cfg.W), &avail);
     if (rc != FF_OK) return rc;
     if (cfg.smem > avail) return set_error(FF_ERR_UNSUPPORTED, "no tile shape for an axis of %d points", n);
-    cfg.grid = (kind == 2 ? nj : ni) * ((p->nh + cfg.W - 1) / cfg.W) * pair;
+    cfg.grid = (kind == 2 ? nj : ni) * ((p->nh + cfg.W - 1) / cfg.W);
   }
   const int ktiles = (p->nh + W - 1) / W;
   // the fused passes hold a whole y tile of 128-byte rows per block (not with
-  // Bluestein axes, 1024-point y lines or narrowed tiles)
-  const bool can_fuse = !any_bs && p->ycfg.N != 1024 && p->ycfg.W == W && p->xcfg.W == W;
+  // Bluestein axes or narrowed tiles)
+  const bool can_fuse = !any_bs && p->ycfg.W == W && p->xcfg.W == W;
   // fused passes: persistent blocks over the in-order tile queue (not with
   // Bluestein axes)
   const int zpp = (nj + 2 * p->zW - 1) / (2 * p->zW);   // z tiles per plane (pairs never cross planes)
