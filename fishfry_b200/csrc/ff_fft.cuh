@@ -25,6 +25,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace ff {
 
 constexpr int kMaxStages = 16;
@@ -315,9 +317,106 @@ struct StageDiv {
   }
 };
 
+// Accessors that can move two adjacent FP32 columns (c, c+1 with c even) as
+// one 16-byte access declare kPair = true and provide ld2/st2.
+template <typename F, typename = void> struct PairAccess : std::false_type {};
+template <typename F>
+struct PairAccess<F, std::void_t<decltype(F::kPair)>> : std::integral_constant<bool, F::kPair> {};
+
+// A point-major FP32 stage with two adjacent columns per item: the pair moves
+// as one 16-byte shared-memory access, and the row group's twiddles are loaded
+// (or generated) once for both columns.  Same arithmetic per value as stage().
+template <int R, bool INV, bool DIT, int W, int NT, int NC, int LC, bool TWREC, int TWMUL, typename LD, typename ST>
+__device__ __forceinline__ void stage_pairs(int n_rt, int L_rt, const AxisDev<float2> &ax, LD &ld, ST &st) {
+  constexpr int WP = W / 2;
+  const int n = NC ? NC : n_rt;
+  const int L = NC ? LC : L_rt;
+  const int m = L / R;
+  const int twstep = TWMUL * n / L;
+  const int nb = n / R;
+  const StageDiv dm(NC ? 1 : m);
+  const bool has_tw = R > 1 && (NC > 0 ? (LC > R) : (L > R));
+  auto body = [&](int it) {
+    const int c = 2 * (it % WP);
+    const int b = it / WP;
+    int blk, j;
+    if (NC) {
+      blk = b / m;
+      j = b - blk * m;
+    } else {
+      blk = dm.quot(b, j);
+    }
+    const int base = blk * L + j;
+    float2 w[R > 1 ? R - 1 : 1];
+    if constexpr (R > 1) {
+      if (has_tw) {
+        if constexpr (TWREC) {
+          double2 w1 = __ldg(ax.tw64 + j * twstep);
+          if (INV) w1.y = -w1.y;
+          double2 ww = w1;
+#pragma unroll
+          for (int r = 1; r < R; r++) {
+            w[r - 1] = to_c(ww, (float2 *)nullptr);
+            if (r + 1 < R) ww = cmul(ww, w1);
+          }
+        } else {
+#pragma unroll
+          for (int r = 1; r < R; r++) {
+            w[r - 1] = __ldg(ax.tw + j * r * twstep);
+            if (INV) w[r - 1].y = -w[r - 1].y;
+          }
+        }
+      }
+    }
+    float2 u[R], v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      const float4 q = ld.ld2(base + r * m, c);
+      u[r] = make_float2(q.x, q.y);
+      v[r] = make_float2(q.z, q.w);
+    }
+    auto apply = [&](float2 *x) {
+#pragma unroll
+      for (int r = 1; r < R; r++) x[r] = cmul(x[r], w[r - 1]);
+    };
+    if (DIT) {
+      if (has_tw) {
+        apply(u);
+        apply(v);
+      }
+      Dft<R, INV, float2>::run(u);
+      Dft<R, INV, float2>::run(v);
+    } else {
+      Dft<R, INV, float2>::run(u);
+      Dft<R, INV, float2>::run(v);
+      if (has_tw) {
+        apply(u);
+        apply(v);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) st.st2(base + r * m, c, make_float4(u[r].x, u[r].y, v[r].x, v[r].y));
+  };
+  if constexpr (NC > 0 && NT > 0 && (WP * (NC / R)) % NT == 0) {
+    constexpr int ITER = WP * (NC / R) / NT;
+#pragma unroll
+    for (int q = 0; q < ITER; q++) body((int)threadIdx.x + q * NT);
+  } else {
+    const int step = NT > 0 ? NT : (int)blockDim.x;
+    for (int it = threadIdx.x; it < WP * nb; it += step) body(it);
+  }
+}
+
 template <int R, bool INV, bool DIT, Map MAP, int W, int NT, int NC, int LC, bool TWREC, int TWMUL = 1, typename C,
           typename LD, typename ST>
 __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, LD &ld, ST &st, int ncols) {
+  // compile-time plans only: a runtime plan instantiates every radix, and the
+  // paired registers of all of them spilled
+  if constexpr (NC > 0 && std::is_same<C, float2>::value && MAP == Map::ColFast && W % 2 == 0 &&
+                PairAccess<LD>::value && PairAccess<ST>::value) {
+    stage_pairs<R, INV, DIT, W, NT, NC, LC, TWREC, TWMUL>(n_rt, L_rt, ax, ld, st);
+    return;
+  }
   const int n = NC ? NC : n_rt;
   const int L = NC ? LC : L_rt;
   const int m = L / R;
@@ -432,8 +531,17 @@ template <typename F> __device__ __forceinline__ void with_radix(int r, F &&f) {
 // Point-major tile: element (pos, c) at sm[pos*W + c].
 template <int W, typename C> struct PointTile {
   C *sm;
+  // columns c, c+1 (c even) of an FP32 tile as one 16-byte access (rows are
+  // 16-byte multiples and the tile 128-byte aligned)
+  static constexpr bool kPair = std::is_same<C, float2>::value && W % 2 == 0;
   __device__ __forceinline__ C operator()(int pos, int c) const { return sm[pos * W + c]; }
   __device__ __forceinline__ void operator()(int pos, int c, C v) const { sm[pos * W + c] = v; }
+  __device__ __forceinline__ float4 ld2(int pos, int c) const {
+    return *reinterpret_cast<const float4 *>(sm + pos * W + c);
+  }
+  __device__ __forceinline__ void st2(int pos, int c, float4 q) const {
+    *reinterpret_cast<float4 *>(sm + pos * W + c) = q;
+  }
 };
 
 // Line-major swizzled tile: element (pos, c) at sm[c*P + swz(pos)]; the

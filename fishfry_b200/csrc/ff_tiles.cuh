@@ -380,6 +380,25 @@ __device__ __forceinline__ unsigned char *align128(unsigned char *p) {
 // y transform of one tile; stage 0 reads through ld0 (the TMA-filled tile or
 // HBM/L2 directly), the last stage stores from registers straight to HBM:
 // frequency row j of the tile's columns goes to row_at(j)[0 .. ncol-1].
+// Store of a strided pass's last stage: frequency row rl(pos) of the tile's
+// columns goes to row_at(row)[c] for c < ncol; FP32 rows also take column
+// pairs as one 16-byte store (rows start 16-byte aligned: the FP32 row pitch
+// is even and tiles start at even columns).
+template <typename C, typename RowAt, typename RL> struct RowStore {
+  const RowAt &row_at;
+  RL rl;
+  int ncol;
+  static constexpr bool kPair = std::is_same<C, float2>::value;
+  __device__ __forceinline__ void operator()(int pos, int c, C v) const {
+    if (c < ncol) row_at(rl(pos))[c] = v;
+  }
+  __device__ __forceinline__ void st2(int pos, int c, float4 q) const {
+    C *p = row_at(rl(pos)) + c;
+    if (c + 1 < ncol) *reinterpret_cast<float4 *>(p) = q;
+    else if (c < ncol) *reinterpret_cast<float2 *>(p) = make_float2(q.x, q.y);
+  }
+};
+
 template <typename T, int W, bool INV, int N, typename LD0, typename RowAt>
 __device__ __forceinline__ void y_tile_rows(LD0 &ld0, const RowAt &row_at, const PassArgs<T> &a, int kt,
                                             typename Cplx<T>::type *sm) {
@@ -388,9 +407,7 @@ __device__ __forceinline__ void y_tile_rows(LD0 &ld0, const RowAt &row_at, const
   const int ncol = min(W, a.nh - kt * W);
   const auto rl = rev_last<N>(ax);
   PointTile<W, C> tile{sm};
-  auto gst = [&](int pos, int c, C v) {
-    if (c < ncol) row_at(rl(pos))[c] = v;
-  };
+  RowStore<C, RowAt, std::remove_const_t<decltype(rl)>> gst{row_at, rl, ncol};
   dif_all<N, INV, Map::ColFast, W, kZThreads, false, (sizeof(T) == 8)>(ax, ld0, tile, gst, W);
 }
 
