@@ -48,8 +48,9 @@ sys.path.insert(0, ROOT)
 L2_BYTES = 126 * 1024 * 1024
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum, bytes per
 # launch) of each pass, from one `ncu --set full` capture of each kernel; the
-# captures' summaries and commands are profiles/passes_fp64_512cube_ncu_full.txt
-# and profiles/passes_fp32_512cube_ncu_full.txt.
+# captures' summaries and commands are profiles/passes_fp64_512cube_ncu_full.txt,
+# profiles/passes_fp32_512cube_ncu_full.txt and
+# profiles/passes_fp64_1024x512x256_ncu_full.txt.
 MEASURED_TRAFFIC = {
     ("512x512x512", "fp64"): {
         "Real-to-complex FFT in Z": 2.10483e9, "Forward FFT in Y": 2.10513e9, "X FFTs and filter": 2.12494e9,
@@ -58,6 +59,10 @@ MEASURED_TRAFFIC = {
     ("512x512x512", "fp32"): {
         "Real-to-complex FFT in Z": 1.03076e9, "Forward FFT in Y": 1.03000e9, "X FFTs and filter": 1.03689e9,
         "Backward FFT in Y": 1.03959e9, "Complex-to-real FFT in Z": 1.03267e9,
+    },
+    ("1024x512x256", "fp64"): {
+        "Real-to-complex FFT in Z": 2.10897e9, "Forward FFT in Y": 2.11055e9, "X FFTs and filter": 2.25110e9,
+        "Backward FFT in Y": 2.11501e9, "Complex-to-real FFT in Z": 2.11054e9,
     },
 }
 
