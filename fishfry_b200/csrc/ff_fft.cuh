@@ -336,9 +336,13 @@ __device__ __forceinline__ void stage_pairs(int n_rt, int L_rt, const AxisDev<fl
   const int nb = n / R;
   const StageDiv dm(NC ? 1 : m);
   const bool has_tw = R > 1 && (NC > 0 ? (LC > R) : (L > R));
+  // the last DIF stage of radix 2 on 64-byte rows: odd items read their rows
+  // swapped (see stage())
+  constexpr bool kSwap = R == 2 && !DIT && W * sizeof(float2) == 64;
   auto body = [&](int it) {
     const int c = 2 * (it % WP);
     const int b = it / WP;
+    const int sw = kSwap && m == 1 ? b & 1 : 0;
     int blk, j;
     if (NC) {
       blk = b / m;
@@ -371,7 +375,7 @@ __device__ __forceinline__ void stage_pairs(int n_rt, int L_rt, const AxisDev<fl
     float2 u[R], v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) {
-      const float4 q = ld.ld2(base + r * m, c);
+      const float4 q = ld.ld2(base + (r ^ sw) * m, c);
       u[r] = make_float2(q.x, q.y);
       v[r] = make_float2(q.z, q.w);
     }
@@ -392,6 +396,10 @@ __device__ __forceinline__ void stage_pairs(int n_rt, int L_rt, const AxisDev<fl
       if (has_tw) {
         apply(u);
         apply(v);
+      }
+      if (sw) {
+        u[R - 1] = make_float2(-u[R - 1].x, -u[R - 1].y);
+        v[R - 1] = make_float2(-v[R - 1].x, -v[R - 1].y);
       }
     }
 #pragma unroll
@@ -489,14 +497,22 @@ __device__ __forceinline__ void stage(int n_rt, int L_rt, const AxisDev<C> &ax, 
       return;
     }
     {
+      // The last DIF stage of radix 2 on a point-major tile of 64-byte rows
+      // (1024-point lines): a quarter warp holds items b and b + 1, whose rows
+      // 2b + r and 2b + 2 + r share banks, so odd items read their two rows
+      // in the other order; the butterfly then gives the same sum and the
+      // negated difference, which is negated back (exact).
+      constexpr bool kSwap = R == 2 && !DIT && MAP == Map::ColFast && W * sizeof(C) == 64;
+      const int sw = kSwap && m == 1 ? b & 1 : 0;
 #pragma unroll
-      for (int r = 0; r < R; r++) v[r] = ld(base + r * m, c);
+      for (int r = 0; r < R; r++) v[r] = ld(base + (r ^ sw) * m, c);
       if (DIT) {
         if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
         Dft<R, INV, C>::run(v);
       } else {
         Dft<R, INV, C>::run(v);
         if (j != 0) apply_twiddles<R, INV, TWREC>(v, j, twstep, ax.tw, ax.tw64);
+        if (sw) v[R - 1] = mk(-v[R - 1].x, -v[R - 1].y);
       }
 #pragma unroll
       for (int r = 0; r < R; r++) st(base + r * m, c, v[r]);

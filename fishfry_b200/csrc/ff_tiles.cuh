@@ -335,12 +335,20 @@ __device__ __forceinline__ void x_filter_stage(int n_rt, LD &ld, ST &st, const X
   using T = typename Real<C>::type;
   const int n = NC ? NC : n_rt;
   const int step = kstep;
+  // Tiles of 64-byte rows (1024-point lines): a quarter warp holds items b and
+  // b + 1, whose rows 2b + r and 2b + 2 + r share banks, so odd items take
+  // their two rows in the other order.  Their forward butterfly then gives the
+  // same sum and the negated difference, the filter scales them by the same
+  // factors, and the inverse butterfly hands back the two outputs swapped,
+  // which the swapped stores put in place: bit-identical values.
+  constexpr bool kSwap = R == 2 && W * sizeof(C) == 64;
   auto body = [&](int it) {
     const int c = it % W;
     const int base = (it / W) * R;
+    const int sw = kSwap ? (it / W) & 1 : 0;
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = ld(base + r, c);
+    for (int r = 0; r < R; r++) v[r] = ld(base + (r ^ sw), c);
     Dft<R, false, C>::run(v);
     const int kh = f.kh0 + c;
     const double kd = double(kh) * f.ddk;
@@ -357,7 +365,7 @@ __device__ __forceinline__ void x_filter_stage(int n_rt, LD &ld, ST &st, const X
     }
     Dft<R, true, C>::run(v);
 #pragma unroll
-    for (int r = 0; r < R; r++) st(base + r, c, v[r]);
+    for (int r = 0; r < R; r++) st(base + (r ^ sw), c, v[r]);
   };
   if constexpr (NC > 0 && (W * (NC / R)) % NT == 0) {
     constexpr int ITER = W * (NC / R) / NT;
