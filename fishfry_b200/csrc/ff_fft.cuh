@@ -577,6 +577,53 @@ template <typename C> struct LineTile {
   __device__ __forceinline__ void operator()(int pos, int c, C v) const { sm[at(pos, c)] = v; }
 };
 
+// Line-major tile of the compile-time z passes: as LineTile, with an XOR
+// swizzle that also folds in higher row bits (t = row of 128 bytes):
+//   FP64 (8 elements per row):  pos ^ ((t ^ t>>3 ^ t>>6) & 7)
+//   FP32 (16 elements per row): pos ^ ((t ^ t<<1 ^ t>>3) & 15)
+// The stages' strided position sets stay conflict free (FP32 ones of stride 8
+// too, which LineTile's swizzle serves in two wavefronts), and so, nearly,
+// do the fused last stages' reads by consecutive frequency bases, whose
+// groups lie at digit-reversed rows (z_split_stage, z_inv_last_stage).
+// Chosen with a bank model over the 64- to 1024-point plans.
+__device__ __forceinline__ int swz_z(int pos, double2 *) {
+  const int t = pos >> 3;
+  return pos ^ ((t ^ (t >> 3) ^ (t >> 6)) & 7);
+}
+__device__ __forceinline__ int swz_z(int pos, float2 *) {
+  const int t = pos >> 4;
+  return pos ^ ((t ^ (t << 1) ^ (t >> 3)) & 15);
+}
+template <typename C> struct LineTileZ {
+  C *sm;
+  int P;
+  __device__ __forceinline__ int at(int pos, int c) const { return c * P + swz_z(pos, (C *)nullptr); }
+  __device__ __forceinline__ C operator()(int pos, int c) const { return sm[at(pos, c)]; }
+  __device__ __forceinline__ void operator()(int pos, int c, C v) const { sm[at(pos, c)] = v; }
+};
+
+// Compile-time plans whose stages before the last are all radix 8 (32, 64,
+// 128, 256, 512, 1024): the last stage's group g (DIF output positions
+// g*RL .. g*RL + RL-1, RL its radix) holds frequencies k0 + r*(N/RL), where
+// k0 is g with its S-1 base-8 digits reversed.  The reversal is its own
+// inverse: group_of_base(k0) is the group whose frequency base is k0.
+__host__ __device__ constexpr bool radix8_prefix(int n) {
+  if (n <= 1 || plan_stages(n) < 2) return false;
+  for (int s = 0; s + 1 < plan_stages(n); s++)
+    if (plan_radix(n, s) != 8) return false;
+  return true;
+}
+template <int N> __device__ __forceinline__ int group_of_base(int k0) {
+  constexpr int D = plan_stages(N) - 1;
+  int g = 0;
+#pragma unroll
+  for (int d = 0; d < D; d++) {
+    g = (g << 3) | (k0 & 7);
+    k0 >>= 3;
+  }
+  return g;
+}
+
 // Digit reversal of a compile-time plan: the frequency held at DIF output
 // position pos (the host builds the same table for runtime plans).
 template <int N> __device__ __forceinline__ int rev_ct(int pos) {

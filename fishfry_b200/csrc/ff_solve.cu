@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zfwd(const T *__restrict__ f, 
       l2_prefetch(f + fl * a.nk, (uint32_t)(min((long)(2 * W), nlines - fl) * a.nk * sizeof(T)));
   }
   const ZTileIO io{&mbar, 0, a.status, a.wait_iters};
-  z_fwd_tile<T, N, BULK, true>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+  z_fwd_tile<T, N, BULK, true, true>(f, spec, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                                reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
 
@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(kZThreads, 3) k_zinv(const typename Cplx<T>::t
                   (uint32_t)(min((long)(2 * W), nlines - fl) * a.nhp * sizeof(typename Cplx<T>::type)));
   }
   const ZTileIO io{&mbar, 0, a.status, a.wait_iters};
-  z_inv_tile<T, N, BULK>(spec, out, a, W, P, (long)blockIdx.x * (2 * W), nlines,
+  z_inv_tile<T, N, BULK, true>(spec, out, a, W, P, (long)blockIdx.x * (2 * W), nlines,
                          reinterpret_cast<typename Cplx<T>::type *>(align128(smraw)), io);
 }
 
@@ -471,9 +471,12 @@ template <typename T> static int configure(ff_plan *p) {
   const size_t per_pair = 2 * (size_t)p->zP * csz;
   p->zW = (int)std::max<size_t>(1, std::min<size_t>(8, (64 * 1024) / per_pair));
   // A: max(W*P, 2W*nhp) values (stages, then output staging), B: W*P values
-  // (+ slack for a copy rounded up to 16 bytes), base alignment
+  // (+ slack for a copy rounded up to 16 bytes), base alignment; where the
+  // forward pass fuses its last stage with the split (z_split_fused) B stages
+  // the output and is as large as A
   const size_t a_bytes = (std::max<size_t>((size_t)p->zW * p->zP, 2 * (size_t)p->zW * p->nhp) * csz + 127) & ~size_t(127);
-  p->zsmem = a_bytes + (size_t)p->zW * p->zP * csz + 128 + 128;
+  const bool zfuse = p->zN > 0 && z_split_fused(p->zN, csz);
+  p->zsmem = a_bytes + (zfuse ? a_bytes : (size_t)p->zW * p->zP * csz) + 128 + 128;
   const long npairs = ((long)ni * nj + 1) / 2;
   p->ztiles = (unsigned)((npairs + p->zW - 1) / p->zW);
   // line blocks by bulk copies: whole 16-byte multiples, and a first stage

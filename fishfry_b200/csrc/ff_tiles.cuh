@@ -51,6 +51,14 @@ template <int N, typename C> __device__ __forceinline__ typename RevLastOf<N>::t
 // Without TMAIO the first stage reads HBM and the output is written from
 // registers.
 // A holds max(W*P, 2W*nhp) complex values, B holds W*P (+ 128 bytes slack).
+//
+// LASTFUSE (single-grid passes, compile-time plans with a radix-8 prefix):
+// the last stage is fused with the split (forward) or with the scatter of the
+// two real lines (inverse), so the stages' output never goes through shared
+// memory in natural order.  Forward: stages in A (LineTileZ), the last stage
+// writes the staged spectrum rows into B, which then also holds
+// max(W*P, 2W*nhp) values.  Inverse: stages in B (LineTileZ), the last stage
+// writes the real lines into A.
 struct ZTileIO {
   uint64_t *mbar;      // TMAIO: barrier of the inbound copy
   uint32_t parity;     // TMAIO: its phase
@@ -97,11 +105,170 @@ __device__ __forceinline__ void bulk_out(E *dst, const E *src, size_t count) {
   }
 }
 
+// Whether the forward z pass of length n fuses its last stage with the split.
+// An item of z_split_stage holds two groups; in FP64 with a radix-8 last
+// stage those need more registers than a thread has (spills, and half the
+// block idle: 0.411 -> 0.437 ms at 512^3), so FP64 512 takes the shuffle form
+// z_split_stage_shfl and FP64 64 (8 bases) keeps the unfused split.
+__host__ __device__ constexpr bool z_split_shfl(int n, size_t csz) {
+  return csz == 16 && radix8_prefix(n) && plan_radix(n, plan_stages(n) - 1) == 8 && n / 8 == 64;
+}
+__host__ __device__ constexpr bool z_split_fused(int n, size_t csz) {
+  return radix8_prefix(n) && (!(csz == 16 && plan_radix(n, plan_stages(n) - 1) == 8) || z_split_shfl(n, csz));
+}
+
+// The last DIF stage of a compile-time z forward transform fused with the R2C
+// split (ParisPencil.cpp:152-165).  An item is the pair of last-stage groups
+// whose frequency bases are k0 and nR - k0 (nR = N/RL), so a thread holds
+// Z[k] and Z[N-k] of its RL frequency pairs in registers and writes
+// A[k] = (Z[k] + conj Z[N-k]) / 2 and B[k] = (Z[k] - conj Z[N-k]) / (2i),
+// k <= N/2, into the staging rows [line][kh] (pitch nhp) of `out`: the rows of
+// the pair's two lines.  Consecutive threads take consecutive k0, so the
+// staging stores are conflict free; LineTileZ spreads the group reads.  The
+// two self-paired bases, 0 and nR/2, come after the others.
+template <int N, typename C>
+__device__ __forceinline__ void z_split_stage(const LineTileZ<C> &t, C *out, int nhp, int W) {
+  using T = typename Real<C>::type;
+  constexpr int S = plan_stages(N);
+  constexpr int RL = plan_radix(N, S - 1);
+  constexpr int nR = N / RL;
+  constexpr int NG = nR / 2 - 1;   // bases 1 .. nR/2 - 1 (with their partners)
+  static_assert(radix8_prefix(N) && nR >= 4, "fused split needs a radix-8 prefix");
+  const T h = (T)0.5;
+  auto emit = [&](int c, int k, C p, C q) {   // p = Z[k], q = Z[N - k]
+    out[(2 * c) * nhp + k] = mk(h * (p.x + q.x), h * (p.y - q.y));
+    out[(2 * c + 1) * nhp + k] = mk(h * (p.y + q.y), h * (q.x - p.x));
+  };
+  for (int it = threadIdx.x; it < W * (NG + 2); it += kZThreads) {
+    if (it < W * NG) {
+      const int c = it / NG;
+      const int k0 = 1 + (it - c * NG);
+      const int g1 = group_of_base<N>(k0), g2 = group_of_base<N>(nR - k0);
+      C z1[RL], z2[RL];
+#pragma unroll
+      for (int r = 0; r < RL; r++) z1[r] = t(g1 * RL + r, c);
+      Dft<RL, false, C>::run(z1);
+#pragma unroll
+      for (int r = 0; r < RL; r++) z2[r] = t(g2 * RL + r, c);
+      Dft<RL, false, C>::run(z2);
+      // z1[r] = Z[k0 + r nR], z2[r] = Z[nR - k0 + r nR]; N - (k0 + r nR) is
+      // the frequency of z2[RL-1-r].  The lower of each pair is k0 + r nR for
+      // r < RL/2 and N - k0 - r nR above.
+#pragma unroll
+      for (int r = 0; r < RL; r++) {
+        if (r < RL / 2) emit(c, k0 + r * nR, z1[r], z2[RL - 1 - r]);
+        else emit(c, N - k0 - r * nR, z2[RL - 1 - r], z1[r]);
+      }
+    } else {
+      const int q = it - W * NG;
+      const int c = q >> 1;
+      const int k0 = (q & 1) ? nR / 2 : 0;
+      const int g = group_of_base<N>(k0);
+      C z[RL];
+#pragma unroll
+      for (int r = 0; r < RL; r++) z[r] = t(g * RL + r, c);
+      Dft<RL, false, C>::run(z);
+      if (k0 == 0) {
+        // frequencies r nR, N - r nR = (RL - r) nR: r = 0 .. RL/2
+#pragma unroll
+        for (int r = 0; r <= RL / 2; r++) emit(c, r * nR, z[r], z[(RL - r) % RL]);
+      } else {
+        // frequencies nR/2 + r nR, N - that = nR/2 + (RL-1-r) nR: r < RL/2
+#pragma unroll
+        for (int r = 0; r < RL / 2; r++) emit(c, nR / 2 + r * nR, z[r], z[RL - 1 - r]);
+      }
+    }
+  }
+}
+
+// The fused last stage and split of the FP64 512-point forward z pass
+// (radix-8 last stage, nR = 64 frequency bases): one group per thread, all
+// threads busy.  A column's 64 groups fill two warps; lane l < 16 holds base
+// k0 and lane l + 16 its partner 64 - k0 (warp 0: k0 = 1..16; warp 1:
+// k0 = 17..31, and the self-paired bases 0 and 32 in lanes 15 and 31).  Each
+// thread needs Z[N - k] for its four outputs k = k0 + r nR (r < 4), which are
+// the partner's upper four values: one exchange of four complex values by
+// warp shuffles.  The base-0 group pairs with itself shifted by one and
+// writes five outputs (0 and N/2 among them).
+template <int N>
+__device__ __forceinline__ void z_split_stage_shfl(const LineTileZ<double2> &t, double2 *out, int nhp, int W) {
+  constexpr int S = plan_stages(N);
+  constexpr int RL = plan_radix(N, S - 1);
+  constexpr int nR = N / RL;
+  static_assert(RL == 8 && nR == 64, "the shuffle split is laid out for 64 bases of radix 8");
+  const double h = 0.5;
+  auto emit = [&](int c, int k, double2 p, double2 q) {   // p = Z[k], q = Z[N - k]
+    out[(2 * c) * nhp + k] = mk(h * (p.x + q.x), h * (p.y - q.y));
+    out[(2 * c + 1) * nhp + k] = mk(h * (p.y + q.y), h * (q.x - p.x));
+  };
+  // W * 64 items are whole warps, so every lane of a warp takes part in the
+  // shuffles of an iteration
+  for (int it = threadIdx.x; it < W * nR; it += kZThreads) {
+    const int c = it >> 6;
+    const int u = it & 63;
+    const int w = u >> 5, l = u & 31;
+    int k0;
+    if (l < 16) k0 = w == 0 ? l + 1 : (l < 15 ? 17 + l : 0);
+    else k0 = w == 0 ? 63 - (l - 16) : (l < 31 ? 47 - (l - 16) : 32);
+    const int g = group_of_base<N>(k0);
+    double2 z[RL];
+#pragma unroll
+    for (int r = 0; r < RL; r++) z[r] = t(g * RL + r, c);
+    Dft<RL, false, double2>::run(z);
+    // partner's upper half: lane l ^ 16, or the thread's own for the two
+    // self-paired bases
+    const bool self = (k0 & 31) == 0;
+    const int src = self ? (int)(threadIdx.x & 31) : (int)((threadIdx.x & 31) ^ 16);
+    double2 q[RL / 2];
+#pragma unroll
+    for (int i = 0; i < RL / 2; i++) {
+      q[i].x = __shfl_sync(0xffffffffu, z[RL / 2 + i].x, src);
+      q[i].y = __shfl_sync(0xffffffffu, z[RL / 2 + i].y, src);
+    }
+    if (k0 != 0) {
+      // N - (k0 + r nR) is the partner's value RL-1-r = q[RL/2-1-r]
+#pragma unroll
+      for (int r = 0; r < RL / 2; r++) emit(c, k0 + r * nR, z[r], q[RL / 2 - 1 - r]);
+    } else {
+      // frequencies r nR pair with (RL - r) nR: r = 0 .. RL/2
+#pragma unroll
+      for (int r = 0; r <= RL / 2; r++) emit(c, r * nR, z[r], z[(RL - r) % RL]);
+    }
+  }
+}
+
+// The last DIF stage of a compile-time z inverse transform fused with the C2R
+// output (ParisPencil.cpp:368-380): item (c, k0) transforms the group whose
+// outputs are the points k0 + r nR and writes their real and imaginary parts
+// to the two real lines of pair c in `raw` (rows of N values).  Consecutive
+// threads take consecutive k0, so the stores are conflict free.
+template <int N, typename C>
+__device__ __forceinline__ void z_inv_last_stage(const LineTileZ<C> &t, typename Real<C>::type *raw, int W) {
+  constexpr int S = plan_stages(N);
+  constexpr int RL = plan_radix(N, S - 1);
+  constexpr int nR = N / RL;
+  static_assert(radix8_prefix(N), "fused last stage needs a radix-8 prefix");
+  for (int it = threadIdx.x; it < W * nR; it += kZThreads) {
+    const int c = it / nR;
+    const int k0 = it - c * nR;
+    const int g = group_of_base<N>(k0);
+    C z[RL];
+#pragma unroll
+    for (int r = 0; r < RL; r++) z[r] = t(g * RL + r, c);
+    Dft<RL, true, C>::run(z);
+#pragma unroll
+    for (int r = 0; r < RL; r++) {
+      raw[(2 * c) * N + k0 + r * nR] = z[r].x;
+      raw[(2 * c + 1) * N + k0 + r * nR] = z[r].y;
+    }
+  }
+}
+
 // R2C along z (ParisPencil.cpp:152-165): the last stage writes Z in natural
 // order into B; the split A[k] = (Z[k] + conj Z[n-k]) / 2,
 // B[k] = (Z[k] - conj Z[n-k]) / (2i) goes out with consecutive threads on
 // consecutive k.
-template <typename T, int N, bool TMAIO, bool TMA_OUT = TMAIO>
+template <typename T, int N, bool TMAIO, bool TMA_OUT = TMAIO, bool LASTFUSE = false>
 __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cplx<T>::type *spec, const PassArgs<T> &a,
                                            int W, int P, long line0, long lend, typename Cplx<T>::type *sm,
                                            const ZTileIO &io) {
@@ -127,6 +294,17 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
       const int la = 2 * c;
       return mk(la < nl ? raw[la * nk + pos] : (T)0, la + 1 < nl ? raw[(la + 1) * nk + pos] : (T)0);
     };
+    if constexpr (LASTFUSE && TMA_OUT && N > 0 && radix8_prefix(N) && z_split_fused(N, sizeof(C))) {
+      // stages in A, the fused last stage stages the spectrum rows in B
+      LineTileZ<C> tAz{A, P};
+      dif_ct<N, plan_stages(N) - 1, 0, false, Map::PosFast, 1, kZThreads, true, true>(ax, ld0, tAz, tAz, W);
+      if constexpr (z_split_shfl(N, sizeof(C))) z_split_stage_shfl<N>(tAz, B, a.nhp, W);
+      else z_split_stage<N>(tAz, B, a.nhp, W);
+      fence_proxy_async_smem();
+      __syncthreads();
+      bulk_out(spec + line0 * a.nhp, B, (size_t)nl * a.nhp);
+      return true;
+    }
     dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ld0, tA, tBrev, W);
     // split into the staging rows [line][kh] (pitch nhp) in A, then one copy out
     const T h = (T)0.5;
@@ -188,7 +366,7 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
 // Hermitian extension in natural order in B (the imaginary parts of the zero
 // and Nyquist terms are dropped, as a C2R transform does), inverse DIF into
 // natural order in B, real and imaginary parts out to the two lines.
-template <typename T, int N, bool TMAIO>
+template <typename T, int N, bool TMAIO, bool LASTFUSE = false>
 __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T *__restrict__ out,
                                            const PassArgs<T> &a, int W, int P, long line0, long lend,
                                            typename Cplx<T>::type *sm, const ZTileIO &io) {
@@ -232,6 +410,17 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
       if (k == 0 || 2 * k == nk) return mk(sa.x, sb.x);
       return lo ? mk(sa.x - sb.y, sa.y + sb.x) : mk(sa.x + sb.y, sb.x - sa.y);
     };
+    if constexpr (LASTFUSE && N > 0 && radix8_prefix(N)) {
+      // stages in B, the fused last stage writes the real lines into A
+      LineTileZ<C> tBz{B, P};
+      dif_ct<N, plan_stages(N) - 1, 0, true, Map::PosFast, 1, kZThreads, true, true>(ax, ldh, tBz, tBz, W);
+      T *rawA = reinterpret_cast<T *>(A);
+      z_inv_last_stage<N>(tBz, rawA, W);
+      fence_proxy_async_smem();
+      __syncthreads();
+      bulk_out(out + line0 * nk, rawA, (size_t)nl * nk);
+      return true;
+    }
     LineTileRev<C, typename RevLastOf<N>::type> tArev{tA, rev_last<N>(ax)};
     dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, ldh, tB, tArev, W);
     // real lines staged in B, then one copy out
