@@ -229,6 +229,9 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
     const int n = XPASS ? a.ni : a.nj;
     if (sh.tma) {
       const CUtensorMap *map = maps + (XPASS ? 1 : 0);
+      // the grid's maps live in global memory and are rewritten when a
+      // server slot changes hands
+      if (threadIdx.x == 0) tensormap_acquire(map);
       if (sh.ct) {
         switch (n) {
 #define FF_CASE(NN) \

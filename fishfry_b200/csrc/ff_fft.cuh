@@ -613,6 +613,18 @@ __host__ __device__ constexpr bool radix8_prefix(int n) {
     if (plan_radix(n, s) != 8) return false;
   return true;
 }
+// Whether the forward z pass of length n fuses its last stage with the split.
+// An item of z_split_stage holds two groups; in FP64 with a radix-8 last
+// stage those need more registers than a thread has (spills, and half the
+// block idle: 0.411 -> 0.437 ms at 512^3), so FP64 512 takes the shuffle form
+// z_split_stage_shfl (ff_tiles.cuh) and FP64 64 (8 bases) keeps the unfused split.
+__host__ __device__ constexpr bool z_split_shfl(int n, size_t csz) {
+  return csz == 16 && radix8_prefix(n) && plan_radix(n, plan_stages(n) - 1) == 8 && n / 8 == 64;
+}
+__host__ __device__ constexpr bool z_split_fused(int n, size_t csz) {
+  return radix8_prefix(n) && (!(csz == 16 && plan_radix(n, plan_stages(n) - 1) == 8) || z_split_shfl(n, csz));
+}
+
 template <int N> __device__ __forceinline__ int group_of_base(int k0) {
   constexpr int D = plan_stages(N) - 1;
   int g = 0;
@@ -760,6 +772,15 @@ __device__ __forceinline__ void mbar_init_fence() {
 // later async-proxy (TMA) accesses of the same memory.
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// A tensor map in global memory (not a kernel parameter) is written by the
+// generic proxy (a copy from the host, possibly over an earlier map at the
+// same address) and read by the TMA unit's tensormap proxy: this acquire
+// fence, by the thread that issues the copies, orders the two, so the TMA
+// does not use a stale descriptor.
+__device__ __forceinline__ void tensormap_acquire(const void *map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
 }
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes) {

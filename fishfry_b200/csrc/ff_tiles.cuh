@@ -105,18 +105,6 @@ __device__ __forceinline__ void bulk_out(E *dst, const E *src, size_t count) {
   }
 }
 
-// Whether the forward z pass of length n fuses its last stage with the split.
-// An item of z_split_stage holds two groups; in FP64 with a radix-8 last
-// stage those need more registers than a thread has (spills, and half the
-// block idle: 0.411 -> 0.437 ms at 512^3), so FP64 512 takes the shuffle form
-// z_split_stage_shfl and FP64 64 (8 bases) keeps the unfused split.
-__host__ __device__ constexpr bool z_split_shfl(int n, size_t csz) {
-  return csz == 16 && radix8_prefix(n) && plan_radix(n, plan_stages(n) - 1) == 8 && n / 8 == 64;
-}
-__host__ __device__ constexpr bool z_split_fused(int n, size_t csz) {
-  return radix8_prefix(n) && (!(csz == 16 && plan_radix(n, plan_stages(n) - 1) == 8) || z_split_shfl(n, csz));
-}
-
 // The last DIF stage of a compile-time z forward transform fused with the R2C
 // split (ParisPencil.cpp:152-165).  An item is the pair of last-stage groups
 // whose frequency bases are k0 and nR - k0 (nR = N/RL), so a thread holds

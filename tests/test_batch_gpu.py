@@ -231,3 +231,60 @@ def test_batch_of_only_side_grids(torch_cuda, ff, oracle):
     batch.solve(d, p, timed=True)
     for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
         assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL, g
+
+
+# the serving test mix plus MIXED: every tile shape the batch kernels choose
+GUARD_DIMS = [(32, 32, 32), (48, 64, 80), (128, 96, 64), (36, 45, 50), (256, 64, 32), (60, 72, 90), (64, 64, 64),
+              (512, 16, 24), (20, 30, 512), (100, 120, 81)] + MIXED
+GUARD = 1 << 16
+SENTINEL = 0xA5
+
+
+def guarded_buffers(torch, sizes, dt):
+    """One device arena per buffer, [guard | buffer | guard] with the guards
+    filled with SENTINEL bytes; returns (arenas, typed views)."""
+    arenas, views = [], []
+    esz = torch.empty(0, dtype=dt).element_size()
+    for nb in sizes:
+        nb_al = (nb + 255) // 256 * 256
+        a = torch.full((GUARD + nb_al + GUARD,), SENTINEL, dtype=torch.uint8, device="cuda")
+        arenas.append((a, nb_al))
+        views.append(a[GUARD:GUARD + nb_al].view(dt)[:nb // esz])
+    return arenas, views
+
+
+def guards_intact(torch, arenas):
+    bad = []
+    for q, (a, nb_al) in enumerate(arenas):
+        lo = a[:GUARD].cpu().numpy()
+        hi = a[GUARD + nb_al:].cpu().numpy()
+        if (lo != SENTINEL).any() or (hi != SENTINEL).any():
+            bad.append((q, int(np.flatnonzero(lo != SENTINEL).size), int(np.flatnonzero(hi != SENTINEL).size)))
+    return bad
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("tuned", [False, True])
+def test_batch_writes_stay_inside_each_grids_buffers(torch_cuda, ff, oracle, precision, tuned):
+    """Every batch kernel writes only its own grid's buffers: guard zones
+    around each density and potential buffer keep their sentinel bytes
+    through a solve (and through the tuner's trial solves), with default and
+    tuned tile shapes."""
+    torch = torch_cuda
+    batch = ff.Batch(GUARD_DIMS, precision=precision)
+    dt = torch.float64 if precision == 0 else torch.float32
+    ad, d = guarded_buffers(torch, batch.nbytes, dt)
+    ap, p = guarded_buffers(torch, batch.nbytes, dt)
+    if tuned:
+        init_all(ff, batch, d, modes_for(ff), precision)
+        batch.tune(d, p, reps=1)
+        torch.cuda.synchronize()
+        assert guards_intact(torch, ad) == [] and guards_intact(torch, ap) == []
+    fs = init_all(ff, batch, d, modes_for(ff), precision)
+    batch.solve(d, p)
+    torch.cuda.synchronize()
+    assert guards_intact(torch, ad) == [], "density guards"
+    assert guards_intact(torch, ap) == [], "potential guards"
+    tol = FP64_TOL if precision == 0 else FP32_TOL
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        assert rel_l2(phi, oracle.solve(f)) <= tol, g

@@ -403,3 +403,33 @@ def test_general_box_in_a_batch(torch_cuda, ff, oracle):
     for g, (f, (lo, hi)) in enumerate(zip(fs, bounds)):
         phi = p[g][:f.size].cpu().numpy().reshape(dims[g])
         assert rel_l2(phi, oracle.solve(f, lo, hi)) <= FP64_TOL, g
+
+
+GUARD = 1 << 16
+SENTINEL = 0xA5
+
+
+@pytest.mark.parametrize("n,precision", [((64, 48, 512), 0), ((48, 64, 512), 1), ((40, 30, 256), 0), ((30, 40, 128), 1),
+                                         ((24, 20, 1024), 0), ((20, 24, 64), 0), ((1024, 8, 10), 0), ((6, 1024, 9), 1),
+                                         ((30, 45, 50), 0), ((97, 13, 30), 0), ((64, 64, 64), 1)])
+def test_solve_writes_stay_inside_its_buffers(torch_cuda, ff, oracle, n, precision):
+    """The single-grid passes write only the plan's two buffers: guard zones
+    around them keep their sentinel bytes through a solve (compile-time z
+    lengths with the fused last stages, 64-byte-row tiles, runtime and
+    Bluestein lengths)."""
+    torch = torch_cuda
+    plan = ff.Plan(n, precision=precision)
+    dt = torch.float64 if precision == ff.FF_FP64 else torch.float32
+    esz = 8 if precision == ff.FF_FP64 else 4
+    nb_al = (plan.nbytes + 255) // 256 * 256
+    arenas = [torch.full((GUARD + nb_al + GUARD,), SENTINEL, dtype=torch.uint8, device="cuda") for _ in range(2)]
+    d, p = [a[GUARD:GUARD + nb_al].view(dt)[:plan.nbytes // esz] for a in arenas]
+    ff.init_field(n, d, None, precision)
+    N = n[0] * n[1] * n[2]
+    f = d[:N].double().cpu().numpy().reshape(n)
+    plan.solve(d, p)
+    torch.cuda.synchronize()
+    for a in arenas:
+        assert (a[:GUARD].cpu().numpy() == SENTINEL).all() and (a[GUARD + nb_al:].cpu().numpy() == SENTINEL).all()
+    phi = p[:N].double().cpu().numpy().reshape(n)
+    assert rel_l2(phi, oracle.solve(f)) <= (FP64_TOL if precision == 0 else FP32_TOL)
