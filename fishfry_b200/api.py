@@ -203,9 +203,16 @@ class Server:
     def submit(self, n, f, precision=FF_FP64, on_host=None):
         """Queue a solve of field f (torch tensor on the device or pinned host
         tensor, or an int device address); returns the request id.  f is kept
-        alive until the request is fetched or released."""
+        alive until the request is fetched or released.  The server's copy of f
+        is ordered after the work on the legacy default stream; a tensor made
+        on another current stream has that stream synchronised first."""
         if on_host is None:
             on_host = not isinstance(f, int) and not f.is_cuda
+        if not isinstance(f, int) and f.is_cuda:
+            import torch
+            cs = torch.cuda.current_stream(f.device)
+            if cs.cuda_stream != 0:
+                cs.synchronize()
         rid = ctypes.c_uint64()
         check(lib().ff_server_submit(self._h, int3(n), int(precision), _ptr(f), int(bool(on_host)), ctypes.byref(rid)),
               "ff_server_submit")

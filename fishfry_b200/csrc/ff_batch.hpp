@@ -78,7 +78,10 @@ inline size_t batch_tile_smem(int kind, int n_axis, int nk, int nhp, int W, size
     const int align = csz == 16 ? 8 : 16;
     const size_t P = (size_t)(nk + align - 1) / align * align;
     const size_t a = std::max<size_t>((size_t)W * P, 2 * (size_t)W * nhp) * csz;
-    return ((a + 127) & ~size_t(127)) + (size_t)W * P * csz + 128 + 128;
+    // a forward tile whose last stage is fused with the split stages the
+    // spectrum rows in its second buffer, which is then as large as the first
+    const size_t b = kind == 0 && z_split_fused(nk, csz) ? ((a + 127) & ~size_t(127)) : (size_t)W * P * csz;
+    return ((a + 127) & ~size_t(127)) + b + 128 + 128;
   }
   return (size_t)n_axis * W * csz + 128;
 }

@@ -183,7 +183,7 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
         switch (a.nk) {
 #define FF_CASE(NN) \
   case NN: {                                                                              \
-    const bool ok = z_fwd_tile<T, NN, true>(g.density, spec, a, zW, P, line0, nlines, sm, io);  \
+    const bool ok = z_fwd_tile<T, NN, true, true, true>(g.density, spec, a, zW, P, line0, nlines, sm, io); \
     parity ^= 1u;                                                                         \
     return ok;                                                                            \
   }
@@ -204,7 +204,7 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
         switch (a.nk) {
 #define FF_CASE(NN)                                                                       \
   case NN: {                                                                              \
-    const bool ok = z_inv_tile<T, NN, true>(spec, g.potential, a, zW, P, line0, nlines, sm, io); \
+    const bool ok = z_inv_tile<T, NN, true, true>(spec, g.potential, a, zW, P, line0, nlines, sm, io); \
     parity ^= 1u;                                                                         \
     return ok;                                                                            \
   }

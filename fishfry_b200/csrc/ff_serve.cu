@@ -104,6 +104,7 @@ struct Request {
   int next_pass = 0;         // passes already scheduled
   long finish_step = -1;     // step whose completion finishes the request
   bool desc_uploaded = false;
+  cudaEvent_t src_ev = nullptr;   // the legacy default stream at submission (the input copy waits for it)
   cudaEvent_t in_ev = nullptr;
   Clock::time_point t_submit, t_admit, t_done;
   BatchGridHost g;
@@ -301,6 +302,10 @@ int admit(ff_server *s) {
     q.g.potential = s->arena_base + q.off_p;
     const size_t esz = q.precision == FF_FP64 ? 8 : 4;
     const size_t fbytes = (size_t)q.n[0] * q.n[1] * q.n[2] * esz;
+    // the copy stream does not synchronise with the legacy default stream:
+    // the input copy waits explicitly for the work queued there before the
+    // submission (a field produced by the caller on that stream)
+    FF_CUDA(cudaStreamWaitEvent(s->copy, q.src_ev, 0));
     FF_CUDA(cudaMemcpyAsync(q.g.density, q.f, fbytes, q.f_on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
                             s->copy));
     if (!q.in_ev) FF_CUDA(cudaEventCreateWithFlags(&q.in_ev, cudaEventDisableTiming));
@@ -495,6 +500,7 @@ template <typename It> static void release_locked(ff_server *s, It it) {
     s->admit_dirty = true;
   }
   if (q.in_ev) cudaEventDestroy(q.in_ev);
+  if (q.src_ev) cudaEventDestroy(q.src_ev);
   s->reqs.erase(it);
 }
 
@@ -555,10 +561,27 @@ int ff_server_submit(ff_server *s, const int n[3], int precision, const void *f,
   q.precision = precision;
   q.f = f;
   q.f_on_host = f_on_host;
+  // mark the legacy default stream of the server's device: the input copy is
+  // ordered after the work the caller queued there before this call
+  {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != s->device) cudaSetDevice(s->device);
+    cudaError_t e = cudaEventCreateWithFlags(&q.src_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(q.src_ev, 0);
+    if (prev >= 0 && prev != s->device) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+      if (q.src_ev) cudaEventDestroy(q.src_ev);
+      return set_error(FF_ERR_CUDA, "ff_server_submit: %s", cudaGetErrorString(e));
+    }
+  }
   q.t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    if (s->fatal != FF_OK) return set_error(s->fatal, "ff_server_submit: server stopped: %s", s->fatal_msg);
+    if (s->fatal != FF_OK) {
+      cudaEventDestroy(q.src_ev);
+      return set_error(s->fatal, "ff_server_submit: server stopped: %s", s->fatal_msg);
+    }
     q.id = s->next_id++;
     *id = q.id;
     if (!s->have_first) {
@@ -752,8 +775,10 @@ int ff_server_destroy(ff_server *s) {
   for (int l = 0; l < 2; l++)
     if (s->lane[l].stream) cudaStreamSynchronize(s->lane[l].stream);
   if (s->copy) cudaStreamSynchronize(s->copy);
-  for (auto &kv : s->reqs)
+  for (auto &kv : s->reqs) {
     if (kv.second.in_ev) cudaEventDestroy(kv.second.in_ev);
+    if (kv.second.src_ev) cudaEventDestroy(kv.second.src_ev);
+  }
   for (auto &kv : s->axes) cudaFree(kv.second.mem);
   for (int l = 0; l < 2; l++) lane_free(s->lane[l]);
   if (s->copy) cudaStreamDestroy(s->copy);

@@ -236,8 +236,11 @@ int ff_server_create(const ff_server_config *cfg, ff_server **server);
 /* Queues a solve of the real field f (ni*nj*nk values of the precision's
  * type, x slowest) on the reference domain of n.  f is a host pointer
  * (f_on_host = 1; pinned memory avoids a staged copy) or a device pointer,
- * and must stay valid until ff_server_wait reports the request done.
- * FF_ERR_NOMEM if the request alone exceeds the budget. */
+ * and must stay valid until ff_server_wait reports the request done.  The
+ * server copies f on its own stream, ordered after the work queued on the
+ * legacy default stream of the server's device before this call; a field
+ * produced on another stream must be complete (that stream synchronised)
+ * before the call.  FF_ERR_NOMEM if the request alone exceeds the budget. */
 int ff_server_submit(ff_server *server, const int n[3], int precision, const void *f, int f_on_host, uint64_t *id);
 
 /* Waits up to timeout_ms (negative, NaN or above 1e12: without limit) for the

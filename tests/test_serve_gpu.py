@@ -178,3 +178,31 @@ def test_server_large_requests_use_tma_tiles_and_match_oracle(torch_cuda, ff, or
             assert rel_l2(phi, oracle.solve(f)) <= tol, n
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("side_stream", [False, True])
+def test_server_input_ordered_after_the_producing_stream(torch_cuda, ff, oracle, side_stream):
+    """A device field whose last write is still queued (behind a long sleep
+    kernel) when it is submitted: the server's input copy waits for it, on
+    the legacy default stream by the submission's event, on another current
+    stream by the wrapper's synchronisation."""
+    torch = torch_cuda
+    n = (64, 48, 40)
+    src = field(torch, ff, n, 0, 21)
+    torch.cuda.synchronize()
+    srv = ff.Server(1 << 30, max_active=16)
+    try:
+        f = torch.zeros_like(src)
+        s = torch.cuda.Stream() if side_stream else torch.cuda.default_stream()
+        with torch.cuda.stream(s):
+            torch.cuda._sleep(100_000_000)   # tens of milliseconds of device time
+            f.copy_(src)
+            rid = srv.submit(n, f, 0)
+        srv.wait(rid)
+        out = torch.empty_like(f)
+        srv.fetch(rid, out)
+        phi = out.double().cpu().numpy().reshape(n)
+        ref = oracle.solve(src.double().cpu().numpy().reshape(n))
+        assert rel_l2(phi, ref) <= FP64_TOL
+    finally:
+        srv.close()
