@@ -616,10 +616,12 @@ __host__ __device__ constexpr bool radix8_prefix(int n) {
 // Whether the forward z pass of length n fuses its last stage with the split.
 // An item of z_split_stage holds two groups; in FP64 with a radix-8 last
 // stage those need more registers than a thread has (spills, and half the
-// block idle: 0.411 -> 0.437 ms at 512^3), so FP64 512 takes the shuffle form
-// z_split_stage_shfl (ff_tiles.cuh) and FP64 64 (8 bases) keeps the unfused split.
+// block idle: 0.411 -> 0.437 ms at 512^3), so 512 points (64 bases) take the
+// shuffle form z_split_stage_shfl (ff_tiles.cuh) in both precisions (FP32:
+// all threads busy and fewer conflicted reads), and FP64 64 (8 bases) keeps
+// the unfused split.
 __host__ __device__ constexpr bool z_split_shfl(int n, size_t csz) {
-  return csz == 16 && radix8_prefix(n) && plan_radix(n, plan_stages(n) - 1) == 8 && n / 8 == 64;
+  return csz > 0 && radix8_prefix(n) && plan_radix(n, plan_stages(n) - 1) == 8 && n / 8 == 64;
 }
 __host__ __device__ constexpr bool z_split_fused(int n, size_t csz) {
   return radix8_prefix(n) && (!(csz == 16 && plan_radix(n, plan_stages(n) - 1) == 8) || z_split_shfl(n, csz));

@@ -169,23 +169,24 @@ __device__ __forceinline__ void z_split_stage(const LineTileZ<C> &t, C *out, int
   }
 }
 
-// The fused last stage and split of the FP64 512-point forward z pass
-// (radix-8 last stage, nR = 64 frequency bases): one group per thread, all
-// threads busy.  A column's 64 groups fill two warps; lane l < 16 holds base
+// The fused last stage and split of the 512-point forward z pass (radix-8
+// last stage, nR = 64 frequency bases): one group per thread, all threads
+// busy.  A column's 64 groups fill two warps; lane l < 16 holds base
 // k0 and lane l + 16 its partner 64 - k0 (warp 0: k0 = 1..16; warp 1:
 // k0 = 17..31, and the self-paired bases 0 and 32 in lanes 15 and 31).  Each
 // thread needs Z[N - k] for its four outputs k = k0 + r nR (r < 4), which are
 // the partner's upper four values: one exchange of four complex values by
 // warp shuffles.  The base-0 group pairs with itself shifted by one and
 // writes five outputs (0 and N/2 among them).
-template <int N>
-__device__ __forceinline__ void z_split_stage_shfl(const LineTileZ<double2> &t, double2 *out, int nhp, int W) {
+template <int N, typename C>
+__device__ __forceinline__ void z_split_stage_shfl(const LineTileZ<C> &t, C *out, int nhp, int W) {
+  using T = typename Real<C>::type;
   constexpr int S = plan_stages(N);
   constexpr int RL = plan_radix(N, S - 1);
   constexpr int nR = N / RL;
   static_assert(RL == 8 && nR == 64, "the shuffle split is laid out for 64 bases of radix 8");
-  const double h = 0.5;
-  auto emit = [&](int c, int k, double2 p, double2 q) {   // p = Z[k], q = Z[N - k]
+  const T h = (T)0.5;
+  auto emit = [&](int c, int k, C p, C q) {   // p = Z[k], q = Z[N - k]
     out[(2 * c) * nhp + k] = mk(h * (p.x + q.x), h * (p.y - q.y));
     out[(2 * c + 1) * nhp + k] = mk(h * (p.y + q.y), h * (q.x - p.x));
   };
@@ -199,15 +200,15 @@ __device__ __forceinline__ void z_split_stage_shfl(const LineTileZ<double2> &t, 
     if (l < 16) k0 = w == 0 ? l + 1 : (l < 15 ? 17 + l : 0);
     else k0 = w == 0 ? 63 - (l - 16) : (l < 31 ? 47 - (l - 16) : 32);
     const int g = group_of_base<N>(k0);
-    double2 z[RL];
+    C z[RL];
 #pragma unroll
     for (int r = 0; r < RL; r++) z[r] = t(g * RL + r, c);
-    Dft<RL, false, double2>::run(z);
+    Dft<RL, false, C>::run(z);
     // partner's upper half: lane l ^ 16, or the thread's own for the two
     // self-paired bases
     const bool self = (k0 & 31) == 0;
     const int src = self ? (int)(threadIdx.x & 31) : (int)((threadIdx.x & 31) ^ 16);
-    double2 q[RL / 2];
+    C q[RL / 2];
 #pragma unroll
     for (int i = 0; i < RL / 2; i++) {
       q[i].x = __shfl_sync(0xffffffffu, z[RL / 2 + i].x, src);
