@@ -520,6 +520,58 @@ __device__ __forceinline__ void x_filter_stage(int n_rt, LD &ld, ST &st, const X
   // factors, and the inverse butterfly hands back the two outputs swapped,
   // which the swapped stores put in place: bit-identical values.
   constexpr bool kSwap = R == 2 && W * sizeof(C) == 64;
+  if constexpr (NC > 0 && std::is_same<C, float2>::value && W % 2 == 0 && PairAccess<LD>::value &&
+                PairAccess<ST>::value) {
+    // FP32, compile-time plan: two adjacent columns per item, loaded as one
+    // 16-byte access; the columns are then finished (filter, inverse
+    // butterfly, 8-byte stores) one after the other, which keeps the pair
+    // within the register budget (both columns to the end spilled)
+    constexpr int WP = W / 2;
+    auto body2 = [&](int it) {
+      const int c = 2 * (it % WP);
+      const int b = it / WP;
+      const int base = b * R;
+      const int sw = kSwap ? b & 1 : 0;
+      float2 u[R], v[R];
+#pragma unroll
+      for (int r = 0; r < R; r++) {
+        const float4 q = ld.ld2(base + (r ^ sw), c);
+        u[r] = make_float2(q.x, q.y);
+        v[r] = make_float2(q.z, q.w);
+      }
+      Dft<R, false, float2>::run(u);
+      Dft<R, false, float2>::run(v);
+      const int k0 = k0_of(base);
+      // one column after the other: filter, inverse butterfly, store
+      auto finish = [&](float2 *x, int cc) {
+        const int kh = f.kh0 + cc;
+        const double kd = double(kh) * f.ddk;
+        const double k2 = kd * kd;
+        const bool live = cc < f.ncol;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const int kx = k0 + r * step;
+          const double id = double(min(kx, f.ni - kx)) * f.ddi;
+          double d = recip_pos((id * id + f.j2) + k2) * f.minvN;
+          if ((kx | f.j | kh) == 0) d = 0.0;
+          if (live) x[r] = cscale(x[r], (float)d);
+        }
+        Dft<R, true, float2>::run(x);
+#pragma unroll
+        for (int r = 0; r < R; r++) st(base + (r ^ sw), cc, x[r]);
+      };
+      finish(u, c);
+      finish(v, c + 1);
+    };
+    if constexpr ((WP * (NC / R)) % NT == 0) {
+      constexpr int ITER = WP * (NC / R) / NT;
+#pragma unroll
+      for (int q = 0; q < ITER; q++) body2((int)threadIdx.x + q * NT);
+    } else {
+      for (int it = threadIdx.x; it < WP * (n / R); it += NT) body2(it);
+    }
+    return;
+  }
   auto body = [&](int it) {
     const int c = it % W;
     const int base = (it / W) * R;
