@@ -100,3 +100,55 @@ def test_slab_rejects_bad_layouts(ff):
         with pytest.raises(ff.FFError) as e:
             SlabKernels(n, lo, hi, ff.FF_FP64, P, 0)
         assert e.value.status == status, (n, P)
+
+
+_NCCL_CHILD = r'''
+import datetime, os, sys
+import numpy as np
+import torch
+import torch.distributed as dist
+sys.path.insert(0, sys.argv[1])
+from fishfry_b200.api import FF_FP64, init_field, reference_domain
+from fishfry_b200.slab import SLAB_PHASES, SlabPencil
+os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=sys.argv[2], RANK="0", WORLD_SIZE="1")
+torch.cuda.set_device(0)
+dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=60), device_id=torch.device("cuda", 0))
+try:
+    n = tuple(int(x) for x in sys.argv[3].split(","))
+    N = n[0] * n[1] * n[2]
+    lo, hi, _, _ = reference_domain(n)
+    sp = SlabPencil(n, lo, hi, (1, 1, 1), (0, 0, 0))
+    nb = sp.bytes()
+    d = torch.zeros(nb // 8, dtype=torch.float64, device="cuda")
+    p = torch.zeros_like(d)
+    init_field(n, d[:N], None, FF_FP64)
+    f = d[:N].cpu().numpy()
+    stamps = []
+    sp.solve(nb, d, p, stamps)
+    assert [s[0] for s in stamps] == ["Total"] + SLAB_PHASES
+    np.save(sys.argv[4], np.stack([f, p[:N].cpu().numpy()]))
+finally:
+    dist.destroy_process_group()
+'''
+
+
+@pytest.mark.parametrize("n", [(64, 48, 40), (30, 45, 50)])
+def test_slab_pencil_over_nccl_on_one_rank(ff, oracle, n, tmp_path):
+    """SlabPencil end to end on a GPU with its default device phases and the
+    exchanges through NCCL's all-to-all (one rank, so each exchange is a copy
+    within the GPU; ranks on several GPUs need a machine with several)."""
+    import os
+    import socket
+    import subprocess
+    import sys
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    out = tmp_path / "slab.npy"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _NCCL_CHILD, root, str(port), ",".join(map(str, n)), str(out)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    f, phi = np.load(out)
+    assert rel_l2(phi.reshape(n), oracle.solve(f.reshape(n))) <= 1e-12
