@@ -433,3 +433,28 @@ def test_solve_writes_stay_inside_its_buffers(torch_cuda, ff, oracle, n, precisi
         assert (a[:GUARD].cpu().numpy() == SENTINEL).all() and (a[GUARD + nb_al:].cpu().numpy() == SENTINEL).all()
     phi = p[:N].double().cpu().numpy().reshape(n)
     assert rel_l2(phi, oracle.solve(f)) <= (FP64_TOL if precision == 0 else FP32_TOL)
+
+
+# z lengths with fused last stages (64 .. 1024), with line counts ni*nj that
+# leave the last z tile partly empty (odd counts, a single line, fewer lines
+# than one tile holds)
+Z_FUSED = [(3, 5, 512), (1, 1, 512), (7, 3, 256), (5, 1, 128), (1, 3, 1024), (3, 1, 64), (9, 7, 32), (2, 3, 512)]
+
+
+@pytest.mark.parametrize("n", Z_FUSED)
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, FP32_TOL)])
+def test_fused_z_lengths_with_partial_tiles(torch_cuda, ff, oracle, n, precision, tol):
+    rng = np.random.default_rng(sum(n) + precision)
+    f = rng.standard_normal(n)
+    plan = ff.Plan(n, precision=precision)
+    dt = torch_cuda.float64 if precision == 0 else torch_cuda.float32
+    esz = 8 if precision == 0 else 4
+    d = torch_cuda.zeros(plan.nbytes // esz, dtype=dt, device="cuda")
+    p = torch_cuda.zeros_like(d)
+    N = n[0] * n[1] * n[2]
+    d[:N] = torch_cuda.from_numpy(f.ravel()).to(dt).cuda()
+    fq = d[:N].double().cpu().numpy().reshape(n)
+    plan.solve(d, p)
+    torch_cuda.cuda.synchronize()
+    phi = p[:N].double().cpu().numpy().reshape(n)
+    assert rel_l2(phi, oracle.solve(fq)) <= tol
