@@ -114,7 +114,7 @@ __device__ __forceinline__ void bulk_out(E *dst, const E *src, size_t count) {
 // the pair's two lines.  Consecutive threads take consecutive k0, so the
 // staging stores are conflict free; LineTileZ spreads the group reads.  The
 // two self-paired bases, 0 and nR/2, come after the others.
-template <int N, typename C>
+template <int N, int NT, typename C>
 __device__ __forceinline__ void z_split_stage(const LineTileZ<C> &t, C *out, int nhp, int W) {
   using T = typename Real<C>::type;
   constexpr int S = plan_stages(N);
@@ -127,7 +127,7 @@ __device__ __forceinline__ void z_split_stage(const LineTileZ<C> &t, C *out, int
     out[(2 * c) * nhp + k] = mk(h * (p.x + q.x), h * (p.y - q.y));
     out[(2 * c + 1) * nhp + k] = mk(h * (p.y + q.y), h * (q.x - p.x));
   };
-  for (int it = threadIdx.x; it < W * (NG + 2); it += kZThreads) {
+  for (int it = threadIdx.x; it < W * (NG + 2); it += NT) {
     if (it < W * NG) {
       const int c = it / NG;
       const int k0 = 1 + (it - c * NG);
@@ -178,7 +178,7 @@ __device__ __forceinline__ void z_split_stage(const LineTileZ<C> &t, C *out, int
 // the partner's upper four values: one exchange of four complex values by
 // warp shuffles.  The base-0 group pairs with itself shifted by one and
 // writes five outputs (0 and N/2 among them).
-template <int N, typename C>
+template <int N, int NT, typename C>
 __device__ __forceinline__ void z_split_stage_shfl(const LineTileZ<C> &t, C *out, int nhp, int W) {
   using T = typename Real<C>::type;
   constexpr int S = plan_stages(N);
@@ -192,7 +192,7 @@ __device__ __forceinline__ void z_split_stage_shfl(const LineTileZ<C> &t, C *out
   };
   // W * 64 items are whole warps, so every lane of a warp takes part in the
   // shuffles of an iteration
-  for (int it = threadIdx.x; it < W * nR; it += kZThreads) {
+  for (int it = threadIdx.x; it < W * nR; it += NT) {
     const int c = it >> 6;
     const int u = it & 63;
     const int w = u >> 5, l = u & 31;
@@ -231,13 +231,13 @@ __device__ __forceinline__ void z_split_stage_shfl(const LineTileZ<C> &t, C *out
 // outputs are the points k0 + r nR and writes their real and imaginary parts
 // to the two real lines of pair c in `raw` (rows of N values).  Consecutive
 // threads take consecutive k0, so the stores are conflict free.
-template <int N, typename C>
+template <int N, int NT, typename C>
 __device__ __forceinline__ void z_inv_last_stage(const LineTileZ<C> &t, typename Real<C>::type *raw, int W) {
   constexpr int S = plan_stages(N);
   constexpr int RL = plan_radix(N, S - 1);
   constexpr int nR = N / RL;
   static_assert(radix8_prefix(N), "fused last stage needs a radix-8 prefix");
-  for (int it = threadIdx.x; it < W * nR; it += kZThreads) {
+  for (int it = threadIdx.x; it < W * nR; it += NT) {
     const int c = it / nR;
     const int k0 = it - c * nR;
     const int g = group_of_base<N>(k0);
@@ -257,7 +257,7 @@ __device__ __forceinline__ void z_inv_last_stage(const LineTileZ<C> &t, typename
 // order into B; the split A[k] = (Z[k] + conj Z[n-k]) / 2,
 // B[k] = (Z[k] - conj Z[n-k]) / (2i) goes out with consecutive threads on
 // consecutive k.
-template <typename T, int N, bool TMAIO, bool TMA_OUT = TMAIO, bool LASTFUSE = false>
+template <typename T, int N, bool TMAIO, bool TMA_OUT = TMAIO, bool LASTFUSE = false, int NT = kZThreads>
 __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cplx<T>::type *spec, const PassArgs<T> &a,
                                            int W, int P, long line0, long lend, typename Cplx<T>::type *sm,
                                            const ZTileIO &io) {
@@ -286,18 +286,18 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
     if constexpr (LASTFUSE && TMA_OUT && N > 0 && radix8_prefix(N) && z_split_fused(N, sizeof(C))) {
       // stages in A, the fused last stage stages the spectrum rows in B
       LineTileZ<C> tAz{A, P};
-      dif_ct<N, plan_stages(N) - 1, 0, false, Map::PosFast, 1, kZThreads, true, true>(ax, ld0, tAz, tAz, W);
-      if constexpr (z_split_shfl(N, sizeof(C))) z_split_stage_shfl<N>(tAz, B, a.nhp, W);
-      else z_split_stage<N>(tAz, B, a.nhp, W);
+      dif_ct<N, plan_stages(N) - 1, 0, false, Map::PosFast, 1, NT, true, true>(ax, ld0, tAz, tAz, W);
+      if constexpr (z_split_shfl(N, sizeof(C))) z_split_stage_shfl<N, NT>(tAz, B, a.nhp, W);
+      else z_split_stage<N, NT>(tAz, B, a.nhp, W);
       fence_proxy_async_smem();
       __syncthreads();
       bulk_out(spec + line0 * a.nhp, B, (size_t)nl * a.nhp);
       return true;
     }
-    dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ld0, tA, tBrev, W);
+    dif_all<N, false, Map::PosFast, 1, NT, true, true>(ax, ld0, tA, tBrev, W);
     // split into the staging rows [line][kh] (pitch nhp) in A, then one copy out
     const T h = (T)0.5;
-    for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+    for (int it = threadIdx.x; it < W * nha; it += NT) {
       const int k = it % nha;
       const int c = it / nha;
       if (k >= nh) continue;
@@ -318,11 +318,11 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
       if (la + 1 < lend) y = f[(la + 1) * nk + pos];
       return mk(x, y);
     };
-    dif_all<N, false, Map::PosFast, 1, kZThreads, true, true>(ax, ldg, tA, tBrev, W);
+    dif_all<N, false, Map::PosFast, 1, NT, true, true>(ax, ldg, tA, tBrev, W);
     const T h = (T)0.5;
     if constexpr (TMA_OUT) {
       // staged rows [line][kh] (pitch nhp) in A, then one copy out
-      for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+      for (int it = threadIdx.x; it < W * nha; it += NT) {
         const int k = it % nha;
         const int c = it / nha;
         if (k >= nh) continue;
@@ -335,7 +335,7 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
       __syncthreads();
       bulk_out(spec + line0 * a.nhp, A, (size_t)nl * a.nhp);
     } else {
-      for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+      for (int it = threadIdx.x; it < W * nha; it += NT) {
         const int k = it % nha;
         const int c = it / nha;
         if (k >= nh) continue;
@@ -355,7 +355,7 @@ __device__ __forceinline__ bool z_fwd_tile(const T *__restrict__ f, typename Cpl
 // Hermitian extension in natural order in B (the imaginary parts of the zero
 // and Nyquist terms are dropped, as a C2R transform does), inverse DIF into
 // natural order in B, real and imaginary parts out to the two lines.
-template <typename T, int N, bool TMAIO, bool LASTFUSE = false>
+template <typename T, int N, bool TMAIO, bool LASTFUSE = false, int NT = kZThreads>
 __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T *__restrict__ out,
                                            const PassArgs<T> &a, int W, int P, long line0, long lend,
                                            typename Cplx<T>::type *sm, const ZTileIO &io) {
@@ -402,19 +402,19 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
     if constexpr (LASTFUSE && N > 0 && radix8_prefix(N)) {
       // stages in B, the fused last stage writes the real lines into A
       LineTileZ<C> tBz{B, P};
-      dif_ct<N, plan_stages(N) - 1, 0, true, Map::PosFast, 1, kZThreads, true, true>(ax, ldh, tBz, tBz, W);
+      dif_ct<N, plan_stages(N) - 1, 0, true, Map::PosFast, 1, NT, true, true>(ax, ldh, tBz, tBz, W);
       T *rawA = reinterpret_cast<T *>(A);
-      z_inv_last_stage<N>(tBz, rawA, W);
+      z_inv_last_stage<N, NT>(tBz, rawA, W);
       fence_proxy_async_smem();
       __syncthreads();
       bulk_out(out + line0 * nk, rawA, (size_t)nl * nk);
       return true;
     }
     LineTileRev<C, typename RevLastOf<N>::type> tArev{tA, rev_last<N>(ax)};
-    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, ldh, tB, tArev, W);
+    dif_all<N, true, Map::PosFast, 1, NT, true, true>(ax, ldh, tB, tArev, W);
     // real lines staged in B, then one copy out
     T *raw = reinterpret_cast<T *>(B);
-    for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
+    for (int it = threadIdx.x; it < W * nk; it += NT) {
       const int t = it % nk;
       const int c = it / nk;
       const C v = tA(t, c);
@@ -426,7 +426,7 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
     bulk_out(out + line0 * nk, raw, (size_t)nl * nk);
     return true;
   } else {
-    for (int it = threadIdx.x; it < W * nha; it += kZThreads) {
+    for (int it = threadIdx.x; it < W * nha; it += NT) {
       const int k = it % nha;
       const int c = it / nha;
       if (k >= nh) continue;
@@ -437,8 +437,8 @@ __device__ __forceinline__ bool z_inv_tile(const typename Cplx<T>::type *spec, T
       hermitian(k, c, sa, sb);
     }
     __syncthreads();
-    dif_all<N, true, Map::PosFast, 1, kZThreads, true, true>(ax, tB, tA, tBrev, W);
-    for (int it = threadIdx.x; it < W * nk; it += kZThreads) {
+    dif_all<N, true, Map::PosFast, 1, NT, true, true>(ax, tB, tA, tBrev, W);
+    for (int it = threadIdx.x; it < W * nk; it += NT) {
       const int t = it % nk;
       const int c = it / nk;
       const long la = line0 + 2 * c;
