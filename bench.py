@@ -53,16 +53,16 @@ L2_BYTES = 126 * 1024 * 1024
 # profiles/passes_fp64_1024x512x256_ncu_full.txt.
 MEASURED_TRAFFIC = {
     ("512x512x512", "fp64"): {
-        "Real-to-complex FFT in Z": 2.10578e9, "Forward FFT in Y": 2.10212e9, "X FFTs and filter": 2.12506e9,
-        "Backward FFT in Y": 2.10398e9, "Complex-to-real FFT in Z": 2.10548e9,
+        "Real-to-complex FFT in Z": 2.10596e9, "Forward FFT in Y": 2.10300e9, "X FFTs and filter": 2.12535e9,
+        "Backward FFT in Y": 2.10666e9, "Complex-to-real FFT in Z": 2.10525e9,
     },
     ("512x512x512", "fp32"): {
-        "Real-to-complex FFT in Z": 1.03102e9, "Forward FFT in Y": 1.02851e9, "X FFTs and filter": 1.02823e9,
-        "Backward FFT in Y": 1.04035e9, "Complex-to-real FFT in Z": 1.03202e9,
+        "Real-to-complex FFT in Z": 1.03033e9, "Forward FFT in Y": 1.02935e9, "X FFTs and filter": 1.02789e9,
+        "Backward FFT in Y": 1.04324e9, "Complex-to-real FFT in Z": 1.03176e9,
     },
     ("1024x512x256", "fp64"): {
-        "Real-to-complex FFT in Z": 2.10876e9, "Forward FFT in Y": 2.11047e9, "X FFTs and filter": 2.25748e9,
-        "Backward FFT in Y": 2.11159e9, "Complex-to-real FFT in Z": 2.10980e9,
+        "Real-to-complex FFT in Z": 2.10856e9, "Forward FFT in Y": 2.11018e9, "X FFTs and filter": 2.25988e9,
+        "Backward FFT in Y": 2.11315e9, "Complex-to-real FFT in Z": 2.11120e9,
     },
 }
 
