@@ -145,18 +145,21 @@ bool batch_shape_valid(int precision, const BatchGridHost &g, int kind, const Ti
   } else if (s.tma && !batch_z_bulk_ok(precision, g.n[2])) {
     return false;
   }
-  return batch_shape_smem(precision, g, kind, s) <= kBatchSmem;
+  return batch_shape_smem(precision, g, kind, s) <= batch_budget(kind);
 }
 
-// Default shape: tiles of about 4096 points (256 threads, a few butterfly
-// items each per stage) within the shared-memory budget; compile-time tiles
-// where the length has them.
+// Default shape: strided tiles of about 4096 points (256 threads) and z tiles
+// of about 2048 (128 threads), a few butterfly items per thread and stage,
+// within the pass's shared-memory budget; compile-time tiles where the
+// length has them.
 TileShape batch_default_shape(int precision, const BatchGridHost &g, int kind) {
   const int n = batch_axis_len(g, kind);
   TileShape s{1, batch_special_n(n) ? 1 : 0, 0};
   if (kind == 0 || kind == 4) {
     const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
-    int W = std::max(1, 2048 / std::max(1, g.n[2]));
+    // about 2048 points per tile: two butterfly items per thread of the
+    // 128-thread z blocks
+    int W = std::max(1, 1024 / std::max(1, g.n[2]));
     W = (int)std::min<long>(W, npairs);
     while (W > 1 && !batch_shape_valid(precision, g, kind, TileShape{W, s.ct, 0})) W--;
     s.W = W;

@@ -22,6 +22,14 @@ namespace ff {
 
 // Per-block shared-memory budget of the batch kernels (three blocks per SM).
 constexpr size_t kBatchSmem = 72 * 1024;
+// The z passes (kinds 0 and 4) run blocks of 128 threads on tiles within
+// 36 KB, six per SM, as the single-grid z passes do: more, smaller tiles in
+// flight hide each block's inbound copy.
+constexpr int kBatchZThreads = 128;
+constexpr size_t kBatchZSmem = 36 * 1024;
+inline int batch_threads(int kind) { return kind == 0 || kind == 4 ? kBatchZThreads : 256; }
+inline size_t batch_budget(int kind) { return kind == 0 || kind == 4 ? kBatchZSmem : kBatchSmem; }
+inline int batch_blocks_per_sm(int kind) { return kind == 0 || kind == 4 ? 6 : 3; }
 
 // Axis lengths with compile-time specialised batch tiles; others use the
 // runtime plan of their axis.
@@ -93,8 +101,8 @@ inline size_t batch_tile_smem(int kind, int n_axis, int nk, int nhp, int W, size
 template <typename T>
 int batch_pass_launch(int kind, const void *grids, const CUtensorMap *maps, const BatchWork &wl, int blocks,
                       size_t smem, cudaStream_t st);
-// Raises the pass kernel's shared-memory limit to kBatchSmem and reports how
-// many blocks of `smem` bytes fit on one SM.
+// Raises the pass kernel's shared-memory limit to its budget (batch_budget)
+// and reports how many blocks of `smem` bytes fit on one SM.
 template <typename T> int batch_pass_prepare(int kind, size_t smem, int *per_sm);
 // Size and alignment of the device grid descriptor for precision T.
 template <typename T> size_t batch_desc_size();

@@ -183,7 +183,7 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
         switch (a.nk) {
 #define FF_CASE(NN) \
   case NN: {                                                                              \
-    const bool ok = z_fwd_tile<T, NN, true, true, true>(g.density, spec, a, zW, P, line0, nlines, sm, io); \
+    const bool ok = z_fwd_tile<T, NN, true, true, true, kBatchZThreads>(g.density, spec, a, zW, P, line0, nlines, sm, io); \
     parity ^= 1u;                                                                         \
     return ok;                                                                            \
   }
@@ -193,18 +193,18 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
         }
       }
       if (sh.tma) {
-        const bool ok = z_fwd_tile<T, 0, true>(g.density, spec, a, zW, P, line0, nlines, sm, io);
+        const bool ok = z_fwd_tile<T, 0, true, true, false, kBatchZThreads>(g.density, spec, a, zW, P, line0, nlines, sm, io);
         parity ^= 1u;
         return ok;
       }
-      return z_fwd_tile<T, 0, false, false>(g.density, spec, a, zW, P, line0, nlines, sm, io);
+      return z_fwd_tile<T, 0, false, false, false, kBatchZThreads>(g.density, spec, a, zW, P, line0, nlines, sm, io);
     } else {
       const C *spec = reinterpret_cast<const C *>(g.density);
       if (sh.ct) {
         switch (a.nk) {
 #define FF_CASE(NN)                                                                       \
   case NN: {                                                                              \
-    const bool ok = z_inv_tile<T, NN, true, true>(spec, g.potential, a, zW, P, line0, nlines, sm, io); \
+    const bool ok = z_inv_tile<T, NN, true, true, kBatchZThreads>(spec, g.potential, a, zW, P, line0, nlines, sm, io); \
     parity ^= 1u;                                                                         \
     return ok;                                                                            \
   }
@@ -214,11 +214,11 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
         }
       }
       if (sh.tma) {
-        const bool ok = z_inv_tile<T, 0, true>(spec, g.potential, a, zW, P, line0, nlines, sm, io);
+        const bool ok = z_inv_tile<T, 0, true, false, kBatchZThreads>(spec, g.potential, a, zW, P, line0, nlines, sm, io);
         parity ^= 1u;
         return ok;
       }
-      return z_inv_tile<T, 0, false>(spec, g.potential, a, zW, P, line0, nlines, sm, io);
+      return z_inv_tile<T, 0, false, false, kBatchZThreads>(spec, g.potential, a, zW, P, line0, nlines, sm, io);
     }
   } else {
     constexpr bool XPASS = KIND == 2;
@@ -260,10 +260,11 @@ __device__ __forceinline__ bool batch_tile(const GridDesc<T> &g, const CUtensorM
 // Persistent pass kernel: blocks take tiles by ticket until the work list is
 // exhausted; the tile's grid is found by binary search over the prefix sums.
 #ifndef FF_BATCH_MINB
-#define FF_BATCH_MINB 3
+#define FF_BATCH_MINB 6
 #endif
 template <typename T, int KIND>
-__global__ void __launch_bounds__(kZThreads, (KIND == 0 || KIND == 4) ? FF_BATCH_MINB : 3)
+__global__ void __launch_bounds__((KIND == 0 || KIND == 4) ? kBatchZThreads : kZThreads,
+                                  (KIND == 0 || KIND == 4) ? FF_BATCH_MINB : 3)
     k_batch(const GridDesc<T> *__restrict__ grids, const CUtensorMap *__restrict__ maps, const BatchWork wl) {
   using C = typename Cplx<T>::type;
   extern __shared__ unsigned char smraw[];
@@ -347,11 +348,11 @@ int batch_pass_launch(int kind, const void *grids, const CUtensorMap *maps, cons
                       size_t smem, cudaStream_t st) {
   const GridDesc<T> *g = static_cast<const GridDesc<T> *>(grids);
   switch (kind) {
-    case 0: k_batch<T, 0><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
-    case 1: k_batch<T, 1><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
-    case 2: k_batch<T, 2><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
-    case 3: k_batch<T, 3><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
-    default: k_batch<T, 4><<<blocks, kZThreads, smem, st>>>(g, maps, wl); break;
+    case 0: k_batch<T, 0><<<blocks, batch_threads(0), smem, st>>>(g, maps, wl); break;
+    case 1: k_batch<T, 1><<<blocks, batch_threads(1), smem, st>>>(g, maps, wl); break;
+    case 2: k_batch<T, 2><<<blocks, batch_threads(2), smem, st>>>(g, maps, wl); break;
+    case 3: k_batch<T, 3><<<blocks, batch_threads(3), smem, st>>>(g, maps, wl); break;
+    default: k_batch<T, 4><<<blocks, batch_threads(4), smem, st>>>(g, maps, wl); break;
   }
   FF_CUDA(cudaGetLastError());
   return FF_OK;
@@ -361,10 +362,10 @@ template <typename T> int batch_pass_prepare(int kind, size_t smem, int *per_sm)
   const void *fn = batch_kernel<T>(kind);
   cudaFuncAttributes fa;
   FF_CUDA(cudaFuncGetAttributes(&fa, fn));
-  if (fa.sharedSizeBytes + kBatchSmem > 227 * 1024)
+  if (fa.sharedSizeBytes + batch_budget(kind) > 227 * 1024)
     return set_error(FF_ERR_UNSUPPORTED, "batch kernel shared memory exceeds the block limit");
-  FF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem));
-  FF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, kZThreads, smem));
+  FF_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)batch_budget(kind)));
+  FF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, batch_threads(kind), smem));
   return FF_OK;
 }
 

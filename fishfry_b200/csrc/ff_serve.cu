@@ -209,8 +209,8 @@ int lane_init(ff_server *s, Lane &L, int precision) {
   for (int q = slots - 1; q >= 0; q--) L.free_slots.push_back(q);
   for (int k = 0; k < 5; k++) {
     int per_sm = 0;
-    int rc = precision == FF_FP64 ? batch_pass_prepare<double>(k, kBatchSmem, &per_sm)
-                                  : batch_pass_prepare<float>(k, kBatchSmem, &per_sm);
+    int rc = precision == FF_FP64 ? batch_pass_prepare<double>(k, batch_budget(k), &per_sm)
+                                  : batch_pass_prepare<float>(k, batch_budget(k), &per_sm);
     if (rc != FF_OK) return rc;
   }
   return FF_OK;
@@ -383,11 +383,11 @@ int issue_step(ff_server *s, Lane &L, bool *issued) {
     const BatchWork wl{reinterpret_cast<const int2 *>(db + e_off[k]), reinterpret_cast<const int *>(db + s_off[k]),
                        cnt[k], reinterpret_cast<int *>(db + t_off) + k};
     const int tiles = reinterpret_cast<int *>(hb + s_off[k])[cnt[k]];
-    const int blocks = std::max(1, std::min(tiles, 3 * s->num_sms));
+    const int blocks = std::max(1, std::min(tiles, batch_blocks_per_sm(k) * s->num_sms));
     cudaStream_t ks = L.kstream[k];
     FF_CUDA(cudaStreamWaitEvent(ks, L.fork_ev, 0));
-    int rc = L.precision == FF_FP64 ? batch_pass_launch<double>(k, L.desc, L.maps, wl, blocks, kBatchSmem, ks)
-                                    : batch_pass_launch<float>(k, L.desc, L.maps, wl, blocks, kBatchSmem, ks);
+    int rc = L.precision == FF_FP64 ? batch_pass_launch<double>(k, L.desc, L.maps, wl, blocks, batch_budget(k), ks)
+                                    : batch_pass_launch<float>(k, L.desc, L.maps, wl, blocks, batch_budget(k), ks);
     if (rc != FF_OK) return rc;
     FF_CUDA(cudaEventRecord(L.kev[k], ks));
     FF_CUDA(cudaStreamWaitEvent(L.stream, L.kev[k], 0));
