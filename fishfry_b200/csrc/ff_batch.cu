@@ -157,9 +157,15 @@ TileShape batch_default_shape(int precision, const BatchGridHost &g, int kind) {
   TileShape s{1, batch_special_n(n) ? 1 : 0, 0};
   if (kind == 0 || kind == 4) {
     const long npairs = ((long)g.n[0] * g.n[1] + 1) / 2;
-    // about 2048 points per tile: two butterfly items per thread of the
-    // 128-thread z blocks
+    // about 2048 points per tile (two butterfly items per thread of the
+    // 128-thread z blocks); longer lines take up to 32 KB of line pairs (at
+    // most 8), as the single-grid z passes do, so that each block moves
+    // enough bytes per copy
+    const size_t csz = precision == FF_FP64 ? 16 : 8;
+    const int align = csz == 16 ? 8 : 16;
+    const size_t per_pair = 2 * (size_t)((g.n[2] + align - 1) / align * align) * csz;
     int W = std::max(1, 1024 / std::max(1, g.n[2]));
+    W = std::max(W, (int)std::max<size_t>(1, std::min<size_t>(8, (32 * 1024) / per_pair)));
     W = (int)std::min<long>(W, npairs);
     while (W > 1 && !batch_shape_valid(precision, g, kind, TileShape{W, s.ct, 0})) W--;
     s.W = W;

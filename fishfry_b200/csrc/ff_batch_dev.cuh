@@ -319,6 +319,26 @@ __global__ void __launch_bounds__((KIND == 0 || KIND == 4) ? kBatchZThreads : kZ
         if (b1 > b0) l2_prefetch(reinterpret_cast<const char *>(G->density) + b0, (uint32_t)(b1 - b0));
       }
     }
+    if constexpr (KIND == 4) {
+      // inverse z pass: the same hint on the spectrum rows of that tile's line
+      // pairs (contiguous, nhp complex values per line, in density)
+      const int t2 = t + (int)gridDim.x;
+      if (threadIdx.x == 32 && t2 < total) {
+        int a2 = lo, b2 = wl.nentry - 1;
+        while (a2 < b2) {
+          const int mid = (a2 + b2 + 1) >> 1;
+          if (__ldg(wl.start + mid) <= t2) a2 = mid;
+          else b2 = mid - 1;
+        }
+        const GridDesc<T> *G = grids + wl.entry[a2].x;
+        const int zW = G->shape[4].W;
+        const long nlines = (long)G->a.ni * G->a.nj;
+        const size_t row = (size_t)G->a.nhp * 2 * sizeof(T);
+        const long l0 = (long)(t2 - __ldg(wl.start + a2)) * 2 * zW;
+        const long l1 = min(l0 + 2 * zW, nlines);
+        if (l1 > l0) l2_prefetch(reinterpret_cast<const char *>(G->density) + (size_t)l0 * row, (uint32_t)((size_t)(l1 - l0) * row));
+      }
+    }
     if (g != last_g) {
       // descriptor of the tile's grid into shared memory (read-only below)
       const int4 *s = reinterpret_cast<const int4 *>(grids + g);
