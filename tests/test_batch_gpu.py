@@ -200,6 +200,24 @@ def test_batch_tma_tiles_for_long_lines(torch_cuda, ff, oracle):
         assert rel_l2(phi, oracle.solve(f)) <= FP64_TOL, (g, dims[g])
 
 
+@pytest.mark.parametrize("precision,tol,want", [(0, FP64_TOL, [4, 5, 25]), (1, FP32_TOL, [8, 8, 25])])
+def test_batch_z_tiles_of_long_lines(torch_cuda, ff, oracle, precision, tol, want):
+    """Default z tiles: about 2048 points for short lines; lines of 256 and
+    200 points take up to 32 KB of line pairs (at most 8), as the single-grid
+    z passes do (FP32 8 pairs, where 2048 points would be 4 and 5)."""
+    # z lengths no tuning test in this process tunes (tuned shapes would
+    # replace the defaults)
+    dims = [(64, 48, 256), (40, 36, 200), (50, 60, 40)]
+    batch = ff.Batch(dims, precision=precision)
+    for g, w in enumerate(want):
+        assert batch.shape(g, 0)[0] == w and batch.shape(g, 4)[0] == w, (g, batch.shape(g, 0), batch.shape(g, 4))
+    d, p = make_buffers(torch_cuda, batch, precision)
+    fs = init_all(ff, batch, d, modes_for(ff, 29), precision)
+    batch.solve(d, p)
+    for g, (f, phi) in enumerate(zip(fs, results(batch, p))):
+        assert rel_l2(phi, oracle.solve(f)) <= tol, (g, dims[g])
+
+
 # Grids the batch kernels do not take (an axis with a prime factor above 7,
 # or longer than their tiles) are solved by their own single-grid plans in
 # the same ff_batch_solve.
